@@ -1,0 +1,449 @@
+// C-ABI of libaccelerint_b200.so: the reference's accelerInt_initialize /
+// accelerInt_integrate / accelerInt_cleanup (generic/solver_interface.cu:88-225)
+// plus run-time selection of solver, mechanism, tolerances and precision.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#include "../../include/accelerint_b200.h"
+#include "kernels.cuh"
+
+using namespace aib;
+
+namespace {
+
+// FMA throughput probe: 8 independent dependency chains per thread.
+template <typename T>
+__global__ void fma_peak_kernel(T* out, int iters, T m) {
+    T a[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = T(threadIdx.x + c) * T(1e-3);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a[c] = fma(a[c], m, T(1e-7));
+    }
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s += a[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+struct MechTablesHost {
+    int K = 0, R = 0;
+    std::vector<double> inv_mw, mw, cp, h_form, s_ref, log_a, beta, ta;
+    std::vector<int4> rsp;
+    std::vector<int> sp_ptr, sp_ent;
+};
+
+struct State {
+    bool initialized = false;
+    int device = 0;
+    int num_sms = 0;
+    int capacity = 0;          // systems per device batch (legacy path)
+    int solver = ACCELERINT_RADAU2A;
+    int mech_kind = 0;         // 0 van der Pol, 1 mass action
+    int lu = ACCELERINT_LU_FP64;
+    double atol = 1e-10, rtol = 1e-6;
+    MechTablesHost mt;
+    MassActionTables dev_tb{};
+    void* dev_tb_mem = nullptr;
+    double* y_dev = nullptr;
+    double* var_dev = nullptr;
+    int* codes_dev = nullptr;
+    int* queue = nullptr;
+    double* jac = nullptr;
+    size_t jac_doubles = 0;
+    cudaStream_t stream = nullptr;
+    int last_status = ACCELERINT_OK;
+    std::vector<int> codes;
+    double poles[4][10] = {};
+};
+
+State g;
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) {                                                               \
+            fprintf(stderr, "accelerint_b200: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(e_), \
+                    __FILE__, __LINE__);                                                       \
+            return ACCELERINT_ERR_CUDA;                                                        \
+        }                                                                                      \
+    } while (0)
+
+int state_n() { return g.mech_kind == 0 ? 2 : g.mt.K + 1; }
+
+int ensure_jac(size_t doubles) {
+    if (doubles <= g.jac_doubles) return ACCELERINT_OK;
+    if (g.jac) cudaFree(g.jac);
+    g.jac = nullptr;
+    g.jac_doubles = 0;
+    CK(cudaMalloc(&g.jac, doubles * sizeof(double)));
+    g.jac_doubles = doubles;
+    return ACCELERINT_OK;
+}
+
+int upload_mass_action() {
+    const MechTablesHost& m = g.mt;
+    if (g.dev_tb_mem) cudaFree(g.dev_tb_mem);
+    g.dev_tb_mem = nullptr;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t nK = size_t(m.K) * sizeof(double), nR = size_t(m.R) * sizeof(double);
+    size_t total = 5 * al(nK) + 3 * al(nR) + al(m.R * sizeof(int4)) + al((m.K + 1) * sizeof(int)) +
+                   al(m.sp_ent.size() * sizeof(int));
+    CK(cudaMalloc(&g.dev_tb_mem, total));
+    char* p = static_cast<char*>(g.dev_tb_mem);
+    auto put = [&](const void* src, size_t bytes) {
+        void* dst = p;
+        cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+        p += al(bytes);
+        return dst;
+    };
+    MassActionTables t;
+    t.K = m.K;
+    t.R = m.R;
+    t.inv_mw = static_cast<const double*>(put(m.inv_mw.data(), nK));
+    t.mw = static_cast<const double*>(put(m.mw.data(), nK));
+    t.cp = static_cast<const double*>(put(m.cp.data(), nK));
+    t.h_form = static_cast<const double*>(put(m.h_form.data(), nK));
+    t.s_ref = static_cast<const double*>(put(m.s_ref.data(), nK));
+    t.log_a = static_cast<const double*>(put(m.log_a.data(), nR));
+    t.beta = static_cast<const double*>(put(m.beta.data(), nR));
+    t.ta = static_cast<const double*>(put(m.ta.data(), nR));
+    t.rsp = static_cast<const int4*>(put(m.rsp.data(), m.R * sizeof(int4)));
+    t.sp_ptr = static_cast<const int*>(put(m.sp_ptr.data(), (m.K + 1) * sizeof(int)));
+    t.sp_ent = static_cast<const int*>(put(m.sp_ent.data(), m.sp_ent.size() * sizeof(int)));
+    CK(cudaGetLastError());
+    g.dev_tb = t;
+    return ACCELERINT_OK;
+}
+
+// ------------------------------------------------------------------ dispatch
+template <class K> int persistent_grid(K kernel, int block, size_t smem, int num_teams_needed, int teams_per_block,
+                                       int* grid) {
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int nb = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, smem));
+    if (nb <= 0) return ACCELERINT_ERR_UNSUPPORTED;
+    const int need = (num_teams_needed + teams_per_block - 1) / teams_per_block;
+    *grid = std::max(1, std::min(nb * g.num_sms, need));
+    return ACCELERINT_OK;
+}
+
+template <int SK, class Mech, int TS, typename LT>
+int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
+    constexpr int N = Mech::N;
+    const int block = 32, tpb = block / TS;
+    const size_t smem = size_t(lay.total) * tpb;
+    auto kern = team_kernel<SK, Mech, TS, LT>;
+    int grid = 0;
+    int rc = persistent_grid(kern, block, smem, a.num, tpb, &grid);
+    if (rc) return rc;
+    rc = ensure_jac(size_t(grid) * tpb * N * N);
+    if (rc) return rc;
+    a.jac = g.jac;
+    CK(cudaMemsetAsync(a.queue, 0, sizeof(int), s));
+    kern<<<grid, block, smem, s>>>(a, mech, lay);
+    CK(cudaGetLastError());
+    return ACCELERINT_OK;
+}
+
+template <int K, int TS>
+int launch_mass_action(BatchArgs a, cudaStream_t s) {
+    using M = MassAction<K>;
+    M mech;
+    mech.tb = g.dev_tb;
+    const int R = g.mt.R;
+    constexpr int N = M::N;
+    if (g.solver == ACCELERINT_RADAU2A) {
+        if (g.lu == ACCELERINT_LU_FP32) {
+            TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R));
+            return launch_team<SK_RADAU, M, TS, float>(a, mech, lay, s);
+        }
+        TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
+        return launch_team<SK_RADAU, M, TS, double>(a, mech, lay, s);
+    }
+    if (g.solver == ACCELERINT_RKC) {
+        TeamLayout lay = TeamLayout::rkc(N, M::smem_rhs(R));
+        return launch_team<SK_RKC, M, TS, double>(a, mech, lay, s);
+    }
+    return ACCELERINT_ERR_UNSUPPORTED;
+}
+
+int launch_vdp(BatchArgs a, cudaStream_t s) {
+    const int block = 128, grid = (a.num + block - 1) / block;
+    if (g.solver == ACCELERINT_RADAU2A) {
+        if (g.lu == ACCELERINT_LU_FP32) tps_kernel<SK_RADAU, VanDerPol, float><<<grid, block, 0, s>>>(a, VanDerPol{});
+        else tps_kernel<SK_RADAU, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
+    } else if (g.solver == ACCELERINT_RKC) {
+        tps_kernel<SK_RKC, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
+    } else {
+        return ACCELERINT_ERR_UNSUPPORTED;
+    }
+    CK(cudaGetLastError());
+    return ACCELERINT_OK;
+}
+
+int launch(BatchArgs a, cudaStream_t s) {
+    if (a.num <= 0) return ACCELERINT_OK;
+    if (g.mech_kind == 0) return launch_vdp(a, s);
+    switch (g.mt.K) {
+        case 13: return launch_mass_action<13, 16>(a, s);
+        case 53: return launch_mass_action<53, 32>(a, s);
+        default: return ACCELERINT_ERR_UNSUPPORTED;
+    }
+}
+
+int run_chunked(int NUM, double t_start, double t_end, double stepsize, double* y_host, const double* var_host) {
+    if (!g.initialized) return ACCELERINT_ERR_STATE;
+    if (NUM < 0 || !y_host || !var_host) return ACCELERINT_ERR_ARGUMENT;
+    const int N = state_n();
+    const double step = stepsize < 0 ? t_end - t_start : stepsize;
+    g.codes.assign(NUM, 0);
+    cudaStream_t s = g.stream;
+    for (int off = 0; off < NUM; off += g.capacity) {
+        const int cnt = std::min(g.capacity, NUM - off);
+        CK(cudaMemcpyAsync(g.var_dev, var_host + off, cnt * sizeof(double), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpy2DAsync(g.y_dev, cnt * sizeof(double), y_host + off, size_t(NUM) * sizeof(double),
+                             cnt * sizeof(double), N, cudaMemcpyHostToDevice, s));
+        BatchArgs a{};
+        a.num = cnt;
+        a.t_start = t_start;
+        a.t_end = t_end;
+        a.step = step;
+        a.y = g.y_dev;
+        a.var = g.var_dev;
+        a.codes = g.codes_dev;
+        a.stats = nullptr;
+        a.queue = g.queue;
+        a.atol = g.atol;
+        a.rtol = g.rtol;
+        int rc = launch(a, s);
+        if (rc) return rc;
+        CK(cudaMemcpy2DAsync(y_host + off, size_t(NUM) * sizeof(double), g.y_dev, cnt * sizeof(double),
+                             cnt * sizeof(double), N, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(g.codes.data() + off, g.codes_dev, cnt * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    for (int c : g.codes)
+        if (c != 0) return ACCELERINT_ERR_SYSTEMS;
+    return ACCELERINT_OK;
+}
+
+int alloc_batch(int capacity) {
+    const int N = state_n();
+    if (g.y_dev) cudaFree(g.y_dev);
+    if (g.var_dev) cudaFree(g.var_dev);
+    if (g.codes_dev) cudaFree(g.codes_dev);
+    g.y_dev = nullptr;
+    g.var_dev = nullptr;
+    g.codes_dev = nullptr;
+    CK(cudaMalloc(&g.y_dev, size_t(capacity) * N * sizeof(double)));
+    CK(cudaMalloc(&g.var_dev, size_t(capacity) * sizeof(double)));
+    CK(cudaMalloc(&g.codes_dev, size_t(capacity) * sizeof(int)));
+    g.capacity = capacity;
+    return ACCELERINT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void accelerInt_initialize(int NUM, int device) {
+    g.last_status = ACCELERINT_OK;
+    device = device < 0 ? 0 : device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device >= ndev) {
+        fprintf(stderr, "accelerint_b200: GPU device %d not available (%d devices)\n", device, ndev);
+        g.last_status = ACCELERINT_ERR_ARGUMENT;
+        return;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) { g.last_status = ACCELERINT_ERR_CUDA; return; }
+    g.device = device;
+    cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (!g.stream) cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
+    if (!g.queue && cudaMalloc(&g.queue, 256) != cudaSuccess) { g.last_status = ACCELERINT_ERR_CUDA; return; }
+    size_t free_mem = 0, total_mem = 0;
+    cudaMemGetInfo(&free_mem, &total_mem);
+    const size_t per = size_t(64 + 2) * sizeof(double) + sizeof(int);
+    const size_t cap = std::min<size_t>(std::max(NUM, 1), size_t(0.5 * double(free_mem) / double(per)));
+    g.initialized = true;
+    if (g.mech_kind == 1 && g.mt.K > 0) {
+        int rc = upload_mass_action();
+        if (rc) { g.last_status = rc; return; }
+    }
+    g.last_status = alloc_batch(int(cap));
+}
+
+void accelerInt_integrate(const int NUM, const double t_start, const double t_end, const double stepsize,
+                          double* y_host, const double* var_host) {
+    g.last_status = run_chunked(NUM, t_start, t_end, stepsize, y_host, var_host);
+}
+
+void accelerInt_cleanup(void) {
+    if (g.y_dev) cudaFree(g.y_dev);
+    if (g.var_dev) cudaFree(g.var_dev);
+    if (g.codes_dev) cudaFree(g.codes_dev);
+    if (g.jac) cudaFree(g.jac);
+    if (g.queue) cudaFree(g.queue);
+    if (g.dev_tb_mem) cudaFree(g.dev_tb_mem);
+    if (g.stream) cudaStreamDestroy(g.stream);
+    g.y_dev = nullptr;
+    g.var_dev = nullptr;
+    g.codes_dev = nullptr;
+    g.jac = nullptr;
+    g.jac_doubles = 0;
+    g.queue = nullptr;
+    g.dev_tb_mem = nullptr;
+    g.stream = nullptr;
+    g.initialized = false;
+    g.capacity = 0;
+}
+
+int accelerInt_set_solver(int solver) {
+    if (solver < ACCELERINT_RADAU2A || solver > ACCELERINT_RKC) return ACCELERINT_ERR_ARGUMENT;
+    g.solver = solver;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_mechanism_van_der_pol(void) {
+    g.mech_kind = 0;
+    if (g.initialized && g.capacity > 0) return alloc_batch(g.capacity);
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_mechanism_mass_action(const accelerInt_mass_action* m) {
+    if (!m || m->n_species < 1 || m->n_species > 63 || m->n_reactions < 1) return ACCELERINT_ERR_ARGUMENT;
+    MechTablesHost t;
+    t.K = m->n_species;
+    t.R = m->n_reactions;
+    for (int k = 0; k < t.K; ++k) {
+        if (!(m->mw[k] > 0)) return ACCELERINT_ERR_ARGUMENT;
+        t.mw.push_back(m->mw[k]);
+        t.inv_mw.push_back(1.0 / m->mw[k]);
+        t.cp.push_back(m->cp[k]);
+        t.h_form.push_back(m->h_form[k]);
+        t.s_ref.push_back(m->s_ref[k]);
+    }
+    std::vector<std::vector<int>> lists(t.K);
+    for (int r = 0; r < t.R; ++r) {
+        int4 q{m->reac[2 * r], m->reac[2 * r + 1], m->prod[2 * r], m->prod[2 * r + 1]};
+        const int sl[4] = {q.x, q.y, q.z, q.w};
+        if (q.x < 0 || q.z < 0) return ACCELERINT_ERR_ARGUMENT;
+        for (int a = 0; a < 4; ++a) {
+            if (sl[a] >= t.K) return ACCELERINT_ERR_ARGUMENT;
+            if (sl[a] >= 0) lists[sl[a]].push_back(4 * r + a);
+        }
+        t.rsp.push_back(q);
+        t.log_a.push_back(m->log_a[r]);
+        t.beta.push_back(m->beta[r]);
+        t.ta.push_back(m->ta[r]);
+    }
+    t.sp_ptr.push_back(0);
+    for (int k = 0; k < t.K; ++k) {
+        for (int e : lists[k]) t.sp_ent.push_back(e);
+        t.sp_ptr.push_back(int(t.sp_ent.size()));
+    }
+    g.mt = t;
+    g.mech_kind = 1;
+    if (g.initialized) {
+        int rc = upload_mass_action();
+        if (rc) return rc;
+        if (g.capacity > 0) return alloc_batch(g.capacity);
+    }
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_tolerances(double atol, double rtol) {
+    if (!(atol > 0) || !(rtol > 0)) return ACCELERINT_ERR_ARGUMENT;
+    g.atol = atol;
+    g.rtol = rtol;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_lu_precision(int precision) {
+    if (precision != ACCELERINT_LU_FP64 && precision != ACCELERINT_LU_FP32) return ACCELERINT_ERR_ARGUMENT;
+    g.lu = precision;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_integrate_status(int NUM, double t_start, double t_end, double stepsize, double* y_host,
+                                const double* var_host) {
+    g.last_status = run_chunked(NUM, t_start, t_end, stepsize, y_host, var_host);
+    return g.last_status;
+}
+
+int accelerInt_integrate_device(int NUM, double t_start, double t_end, double stepsize, double* y_dev,
+                                const double* var_dev, int* codes_dev, int* stats_dev, void* stream) {
+    if (!g.initialized) return ACCELERINT_ERR_STATE;
+    if (NUM < 0 || (NUM > 0 && (!y_dev || !var_dev))) return ACCELERINT_ERR_ARGUMENT;
+    BatchArgs a{};
+    a.num = NUM;
+    a.t_start = t_start;
+    a.t_end = t_end;
+    a.step = stepsize < 0 ? t_end - t_start : stepsize;
+    a.y = y_dev;
+    a.var = var_dev;
+    a.codes = codes_dev;
+    a.stats = stats_dev;
+    a.queue = g.queue;
+    a.atol = g.atol;
+    a.rtol = g.rtol;
+    return launch(a, static_cast<cudaStream_t>(stream));
+}
+
+int accelerInt_last_status(void) { return g.last_status; }
+
+int accelerInt_get_codes(int* codes_host, int NUM) {
+    if (!codes_host || NUM < 0 || size_t(NUM) > g.codes.size()) return ACCELERINT_ERR_ARGUMENT;
+    std::memcpy(codes_host, g.codes.data(), size_t(NUM) * sizeof(int));
+    return ACCELERINT_OK;
+}
+
+int accelerInt_get_poles(double* pr, double* pi, double* rr, double* ri) {
+    if (!pr || !pi || !rr || !ri) return ACCELERINT_ERR_ARGUMENT;
+    for (int i = 0; i < 10; ++i) {
+        pr[i] = g.poles[0][i];
+        pi[i] = g.poles[1][i];
+        rr[i] = g.poles[2][i];
+        ri[i] = g.poles[3][i];
+    }
+    return ACCELERINT_OK;
+}
+
+const char* accelerInt_version(void) { return "accelerint_b200 0.1 (sm_100a)"; }
+
+int accelerInt_measure_fma_peak(int fp64, double* tflops) {
+    if (!tflops) return ACCELERINT_ERR_ARGUMENT;
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    void* out = nullptr;
+    const int block = 256, grid = sms * 8, iters = 4096;
+    CK(cudaMalloc(&out, size_t(grid) * block * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(e0);
+        if (fp64) fma_peak_kernel<double><<<grid, block>>>(static_cast<double*>(out), iters, 1.0000001);
+        else fma_peak_kernel<float><<<grid, block>>>(static_cast<float*>(out), iters, 1.0000001f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    CK(cudaGetLastError());
+    const double flops = 2.0 * 8.0 * double(iters) * grid * block;   // 8 independent chains per thread
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return ACCELERINT_OK;
+}
+
+}  // extern "C"

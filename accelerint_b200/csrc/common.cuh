@@ -1,0 +1,136 @@
+// Common device building blocks: teams of lanes that own one system, complex
+// arithmetic, reductions.  sm_100a only.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cfloat>
+
+namespace aib {
+
+// Return codes of the integrators (radau2a/radau2a_props.h:288-296,
+// exprb43_props.h:356-362, rkc_props.h:427).
+enum : int {
+    EC_success = 0,
+    EC_consecutive_steps = 1,
+    EC_max_steps_exceeded = 2,
+    EC_h_plus_t_equals_h = 3,
+    EC_newton_max_iterations_exceeded = 4,
+};
+
+// Per-system counters (stats_dev[ivp * NSTATS + k]).
+enum : int {
+    ST_STEPS = 0, ST_ACCEPT, ST_REJECT, ST_JAC, ST_DECOMP, ST_NEWTON, ST_RHS, ST_AUX, NSTATS
+};
+
+struct Stats {
+    int c[NSTATS];
+    __device__ void clear() {
+#pragma unroll
+        for (int i = 0; i < NSTATS; ++i) c[i] = 0;
+    }
+};
+
+// ------------------------------------------------------------------ complex
+template <typename T> struct cx { T re, im; };
+using cxd = cx<double>;
+
+template <typename T> __device__ __forceinline__ cx<T> cmake(T r, T i) { return {r, i}; }
+template <typename T> __device__ __forceinline__ cx<T> cadd(cx<T> a, cx<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename T> __device__ __forceinline__ cx<T> csub(cx<T> a, cx<T> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename T> __device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+// a - b * c
+template <typename T> __device__ __forceinline__ cx<T> cfnma(cx<T> b, cx<T> c, cx<T> a) {
+    return {a.re - b.re * c.re + b.im * c.im, a.im - b.re * c.im - b.im * c.re};
+}
+template <typename T> __device__ __forceinline__ T cabs1(cx<T> a) { return fabs(a.re) + fabs(a.im); }
+// 1 / b by Smith's scaling (R. L. Smith, CACM 5(8), 1962)
+template <typename T> __device__ __forceinline__ cx<T> crecip(cx<T> b) {
+    if (fabs(b.re) >= fabs(b.im)) {
+        T r = b.im / b.re, d = b.re + b.im * r;
+        return {T(1) / d, -r / d};
+    } else {
+        T r = b.re / b.im, d = b.re * r + b.im;
+        return {r / d, T(-1) / d};
+    }
+}
+// a / b by Smith's algorithm
+template <typename T> __device__ __forceinline__ cx<T> cdiv(cx<T> a, cx<T> b) {
+    if (fabs(b.re) >= fabs(b.im)) {
+        T r = b.im / b.re, d = b.re + b.im * r;
+        return {(a.re + a.im * r) / d, (a.im - a.re * r) / d};
+    } else {
+        T r = b.re / b.im, d = b.re * r + b.im;
+        return {(a.re * r + a.im) / d, (a.im * r - a.re) / d};
+    }
+}
+
+// ------------------------------------------------------------------ teams
+// A team of TS consecutive lanes of one warp integrates one system.  TS = 1 is
+// a thread per system (everything in registers); TS = 16 or 32 share the
+// system's matrices in shared memory.  Control decisions must be identical on
+// every lane of a team, so every reduction ends with a broadcast of one lane's
+// value (a butterfly alone can leave lanes with differently rounded sums).
+template <int TS> struct Team {
+    static_assert(TS == 1 || TS == 2 || TS == 4 || TS == 8 || TS == 16 || TS == 32, "team size");
+    static constexpr int size = TS;
+    __device__ __forceinline__ static int lane() { return TS == 1 ? 0 : int(threadIdx.x & (TS - 1)); }
+    __device__ __forceinline__ static unsigned mask() {
+        if (TS == 32) return 0xffffffffu;
+        if (TS == 1) return 1u << (threadIdx.x & 31);
+        const unsigned base = (threadIdx.x & 31) & ~unsigned(TS - 1);
+        return ((1u << TS) - 1u) << base;
+    }
+    __device__ __forceinline__ static void sync() {
+        if (TS > 1) __syncwarp(mask());
+    }
+    __device__ __forceinline__ static double bcast(double v, int src) {
+        if (TS == 1) return v;
+        return __shfl_sync(mask(), v, src, TS);
+    }
+    __device__ __forceinline__ static int bcast(int v, int src) {
+        if (TS == 1) return v;
+        return __shfl_sync(mask(), v, src, TS);
+    }
+    __device__ __forceinline__ static double sum(double v) {
+        if (TS == 1) return v;
+#pragma unroll
+        for (int o = TS / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask(), v, o, TS);
+        return __shfl_sync(mask(), v, 0, TS);
+    }
+    __device__ __forceinline__ static double max(double v) {
+        if (TS == 1) return v;
+#pragma unroll
+        for (int o = TS / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask(), v, o, TS));
+        return __shfl_sync(mask(), v, 0, TS);
+    }
+    // argmax of v with ties to the smallest index; returns the index on every lane
+    __device__ __forceinline__ static int argmax(double v, int idx) {
+        if (TS == 1) return idx;
+#pragma unroll
+        for (int o = TS / 2; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(mask(), v, o, TS);
+            int oi = __shfl_xor_sync(mask(), idx, o, TS);
+            if (ov > v || (ov == v && oi < idx) || (v != v && ov == ov)) { v = ov; idx = oi; }
+        }
+        return __shfl_sync(mask(), idx, 0, TS);
+    }
+};
+
+// A length-N vector distributed over a team: lane l owns elements l, l + TS, ...
+template <int N, int TS> struct Vec {
+    static constexpr int S = (N + TS - 1) / TS;
+    double v[S];
+    __device__ __forceinline__ static int idx(int s) { return Team<TS>::lane() + TS * s; }
+    __device__ __forceinline__ static bool ok(int s) { return (N % TS == 0) || idx(s) < N; }
+    __device__ __forceinline__ double& operator[](int s) { return v[s]; }
+    __device__ __forceinline__ const double& operator[](int s) const { return v[s]; }
+};
+
+template <int N, int TS> __device__ __forceinline__ void vfill(Vec<N, TS>& a, double x) {
+#pragma unroll
+    for (int s = 0; s < Vec<N, TS>::S; ++s) a[s] = x;
+}
+
+}  // namespace aib

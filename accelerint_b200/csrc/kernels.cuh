@@ -1,0 +1,182 @@
+// Batch kernels: the device side of accelerInt_integrate.
+//
+// The reference launches one thread per system over a padded grid
+// (generic/solver_generic.cu:28-42, solver_interface.cu:189).  Here:
+//   * thread-per-system kernels for the 2-state van der Pol workload, state in
+//     registers, coalesced structure-of-arrays loads y[i*num + ivp];
+//   * persistent team kernels for the mass-action mechanisms: one team of TS
+//     lanes per system, its matrices in shared memory; teams pull systems from
+//     a device work queue (one atomic per system), so systems with very
+//     different stiffness do not hold each other up.
+// Every kernel integrates all global steps [t_k, t_{k+1}] of its systems in
+// one launch; each step restarts the integrator exactly as a separate
+// intDriver call of the reference would.
+#pragma once
+#include "common.cuh"
+#include "mech.cuh"
+#include "radau2a.cuh"
+#include "rkc.cuh"
+
+namespace aib {
+
+struct BatchArgs {
+    int num;
+    double t_start, t_end, step;
+    double* y;              // [N * num] column-major, IVP fastest
+    const double* var;      // [num]
+    int* codes;             // [num] or null
+    int* stats;             // [num * NSTATS] or null
+    int* queue;             // work-queue counter (zeroed before launch)
+    double* jac;            // per-team Jacobian scratch [teams * N * N]
+    double atol, rtol;
+};
+
+// The reference's global-step loop (generic/solver_main.c:196-209), measured from t_start.
+struct StepLoop {
+    double t, t_next, t_start, t_end, step;
+    int k;
+    __device__ StepLoop(double a, double b, double s) : t(a), t_start(a), t_end(b), step(s), k(0) {
+        t_next = fmin(t_end, t_start + step);
+    }
+    __device__ bool more() const { return t + DBL_EPSILON < t_end; }
+    __device__ void advance() {
+        ++k;
+        t = t_next;
+        t_next = fmin(t_end, t_start + double(k + 1) * step);
+    }
+};
+
+template <int N, int TS>
+__device__ __forceinline__ void store_stats(const BatchArgs& a, int sys, const Stats& st) {
+    if (a.stats && Team<TS>::lane() == 0) {
+        int* o = a.stats + size_t(sys) * NSTATS;
+#pragma unroll
+        for (int k = 0; k < NSTATS; ++k) o[k] += st.c[k];
+    }
+}
+
+// ------------------------------------------------------------- thread per system
+enum SolverKind { SK_RADAU = 0, SK_EXPRB43 = 1, SK_EXP4 = 2, SK_RKC = 3 };
+
+template <int SK, class Mech, typename LT>
+__global__ void __launch_bounds__(128) tps_kernel(BatchArgs a, Mech mech)
+{
+    constexpr int N = Mech::N;
+    const int sys = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sys >= a.num) return;
+    Vec<N, 1> y;
+#pragma unroll
+    for (int i = 0; i < N; ++i) y[i] = a.y[size_t(i) * a.num + sys];
+    const double pr = a.var[sys];
+    Stats st;
+    st.clear();
+    int code = EC_success;
+    StepLoop L(a.t_start, a.t_end, a.step);
+    if constexpr (SK == SK_RADAU) {
+        RadauRegStore<N, LT> store;
+        Radau<N, 1, Mech, LT, RadauRegStore<N, LT>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
+        while (L.more() && code == EC_success) {
+            code = rad.integrate(L.t, L.t_next, y);
+            L.advance();
+        }
+    } else if constexpr (SK == SK_RKC) {
+        Rkc<N, 1, Mech> rk{mech, nullptr, a.atol, a.rtol, pr, st};
+        while (L.more() && code == EC_success) {
+            code = rk.integrate(L.t, L.t_next, y);
+            L.advance();
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) a.y[size_t(i) * a.num + sys] = y[i];
+    if (a.codes) a.codes[sys] = code;
+    store_stats<N, 1>(a, sys, st);
+}
+
+// ------------------------------------------------------------- team per system
+// Shared-memory layout of one team (bytes, 16-byte aligned pieces).
+struct TeamLayout {
+    int e1, e2, d1, d2, p1, p2, buf, rhs, total;
+    __host__ __device__ static int al(int b) { return (b + 15) & ~15; }
+    __host__ __device__ static TeamLayout radau(int N, int lt_bytes, int rhs_doubles, int jac_doubles) {
+        TeamLayout L;
+        int o = 0;
+        L.e1 = o; o += al(N * N * lt_bytes);
+        L.e2 = o;
+        const int e2b = N * N * 2 * lt_bytes, jb = jac_doubles * 8;
+        o += al(e2b > jb ? e2b : jb);
+        L.d1 = o; o += al(N * lt_bytes);
+        L.d2 = o; o += al(N * 2 * lt_bytes);
+        L.p1 = o; o += al(N * 4);
+        L.p2 = o; o += al(N * 4);
+        L.buf = o; o += al(N * 8);
+        L.rhs = o; o += al(rhs_doubles * 8);
+        L.total = o;
+        return L;
+    }
+    __host__ __device__ static TeamLayout rkc(int N, int rhs_doubles) {
+        TeamLayout L{};
+        L.buf = 0;
+        L.rhs = al(N * 8);
+        L.total = L.rhs + al(rhs_doubles * 8);
+        return L;
+    }
+};
+
+template <int SK, class Mech, int TS, typename LT>
+__global__ void __launch_bounds__(32) team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
+{
+    constexpr int N = Mech::N;
+    using TM = Team<TS>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tib = threadIdx.x / TS;
+    const int tpb = blockDim.x / TS;
+    const int gteam = blockIdx.x * tpb + tib;
+    unsigned char* base = smem + size_t(tib) * lay.total;
+    const int lane = TM::lane();
+    for (;;) {
+        int sys = 0;
+        if (lane == 0) sys = atomicAdd(a.queue, 1);
+        sys = TM::bcast(sys, 0);
+        if (sys >= a.num) break;
+        Vec<N, TS> y;
+#pragma unroll
+        for (int s = 0; s < Vec<N, TS>::S; ++s)
+            y[s] = Vec<N, TS>::ok(s) ? a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] : 0.0;
+        const double pr = a.var[sys];
+        Stats st;
+        st.clear();
+        int code = EC_success;
+        StepLoop L(a.t_start, a.t_end, a.step);
+        if constexpr (SK == SK_RADAU) {
+            RadauTeamStore<N, LT> store;
+            store.J = a.jac + size_t(gteam) * N * N;
+            store.E1 = reinterpret_cast<LT*>(base + lay.e1);
+            store.E2 = reinterpret_cast<cx<LT>*>(base + lay.e2);
+            store.d1 = reinterpret_cast<LT*>(base + lay.d1);
+            store.d2 = reinterpret_cast<cx<LT>*>(base + lay.d2);
+            store.p1 = reinterpret_cast<int*>(base + lay.p1);
+            store.p2 = reinterpret_cast<int*>(base + lay.p2);
+            store.buf = reinterpret_cast<double*>(base + lay.buf);
+            store.rhs = reinterpret_cast<double*>(base + lay.rhs);
+            Radau<N, TS, Mech, LT, RadauTeamStore<N, LT>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
+            while (L.more() && code == EC_success) {
+                code = rad.integrate(L.t, L.t_next, y);
+                L.advance();
+            }
+        } else if constexpr (SK == SK_RKC) {
+            Rkc<N, TS, Mech> rk{mech, reinterpret_cast<double*>(base + lay.rhs), a.atol, a.rtol, pr, st};
+            while (L.more() && code == EC_success) {
+                code = rk.integrate(L.t, L.t_next, y);
+                L.advance();
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < Vec<N, TS>::S; ++s)
+            if (Vec<N, TS>::ok(s)) a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] = y[s];
+        if (a.codes && lane == 0) a.codes[sys] = code;
+        store_stats<N, TS>(a, sys, st);
+        TM::sync();
+    }
+}
+
+}  // namespace aib

@@ -1,0 +1,435 @@
+// Radau IIA (3-stage, order 5) for one system per team, after
+// radau2a/radau2a.c:520-736 (CPU reference; the GPU reference radau2a.cu has
+// the RK_ErrorEstimate bug of solving with the raw Jacobian, radau2a.cu:612,
+// which is not reproduced).
+//
+// Same control logic, constants and operation sequence as the CPU reference:
+// simplified Newton with the real E1 and complex E2 factorisations, Gustafsson
+// step control, Jacobian / LU reuse (SkipJac / SkipLU), quadratic-interpolant
+// starting values (including the reference's x2 factor in Z3, radau2a.c:312).
+// The matrices are factorised in precision LT (double, or float for the
+// precision form where the Newton loop itself refines the solution and the
+// error-estimate solve gets one FP64 refinement step against J).
+#pragma once
+#include "common.cuh"
+#include "linalg.cuh"
+
+namespace aib {
+
+namespace radau {
+// radau2a.c:38-65
+constexpr int MAX_NO_STEPS = 200000;
+constexpr int NEWTON_MAXIT = 8;
+constexpr double ROUNDOFF = DBL_EPSILON;
+constexpr double FAC_MIN = 0.2, FAC_MAX = 8, FAC_SAFE = 0.9, FAC_REJ = 0.1;
+constexpr double THETA_MIN = 0.001, NEWTON_TOL = 0.03, Q_MIN = 1.0, Q_MAX = 1.2;
+constexpr int MAX_CONSECUTIVE_ERRS = 5;
+// radau2a.c:101-229
+__host__ __device__ constexpr double A(int i, int j) {
+    constexpr double v[3][3] = {
+    {1.968154772236604258683861429918299e-1, -6.55354258501983881085227825696087e-2,
+     2.377097434822015242040823210718965e-2},
+    {3.944243147390872769974116714584975e-1, 2.920734116652284630205027458970589e-1,
+     -4.154875212599793019818600988496743e-2},
+    {3.764030627004672750500754423692808e-1, 5.124858261884216138388134465196080e-1,
+     1.111111111111111111111111111111111e-1}};
+    return v[i][j];
+}
+__host__ __device__ constexpr double C(int i) {
+    constexpr double v[3] = {1.550510257216821901802715925294109e-1, 6.449489742783178098197284074705891e-1, 1.0};
+    return v[i];
+}
+__host__ __device__ constexpr double E(int i) {
+    constexpr double v[4] = {0.05, -10.04880939982741556246032950764708 * 0.05,
+                         1.382142733160748895793662840980412 * 0.05, -0.3333333333333333333333333333333333 * 0.05};
+    return v[i];
+}
+constexpr double GAMMA = 3.637834252744495732208418513577775;
+constexpr double ALPHA = 2.681082873627752133895790743211112;
+constexpr double BETA = 3.050430199247410569426377624787569;
+__host__ __device__ constexpr double T(int i, int j) {
+    constexpr double v[3][3] = {
+    {9.443876248897524148749007950641664e-2, -1.412552950209542084279903838077973e-1,
+     -3.00291941051474244918611170890539e-2},
+    {2.502131229653333113765090675125018e-1, 2.041293522937999319959908102983381e-1,
+     3.829421127572619377954382335998733e-1},
+    {1.0, 1.0, 0.0e0}};
+    return v[i][j];
+}
+__host__ __device__ constexpr double TIA(int i, int j) {
+    constexpr double v[3][3] = {
+    {1.520148562492775501049204957366528e+1, 1.192055789400527921212348994770778,
+     1.903956760517560343018332287285119},
+    {-9.669512977505946748632625374449567, -8.724028436822336183071773193986487,
+     3.096043239482439656981667712714881},
+    {-1.409513259499574544876303981551774e+1, 5.895975725255405108079130152868952,
+     -1.441236197545344702389881889085515e-1}};
+    return v[i][j];
+}
+constexpr double ELO = 4;
+}  // namespace radau
+
+// Matrix storage of one team: shared memory for teams of several lanes (J may
+// live in global scratch), registers/local memory for a thread per system.
+template <int N, typename LT> struct RadauRegStore {
+    double J[N * N];
+    LT E1[N * N];
+    cx<LT> E2[N * N];
+    LT d1[N];
+    cx<LT> d2[N];
+    int p1[N], p2[N];
+    double buf[N];
+    __device__ double* jac() { return J; }
+    __device__ LT* e1() { return E1; }
+    __device__ cx<LT>* e2() { return E2; }
+    __device__ LT* dinv1() { return d1; }
+    __device__ cx<LT>* dinv2() { return d2; }
+    __device__ int* perm1() { return p1; }
+    __device__ int* perm2() { return p2; }
+    __device__ double* vbuf() { return buf; }
+    __device__ double* scratch_rhs() { return nullptr; }
+    __device__ double* scratch_jac() { return nullptr; }
+};
+
+template <int N, typename LT> struct RadauTeamStore {
+    double* J;        // N*N (global scratch)
+    LT* E1;           // N*N
+    cx<LT>* E2;       // N*N (also the Jacobian evaluation scratch)
+    LT* d1;
+    cx<LT>* d2;
+    int* p1;
+    int* p2;
+    double* buf;      // N
+    double* rhs;      // mechanism dydt scratch
+    __device__ double* jac() { return J; }
+    __device__ LT* e1() { return E1; }
+    __device__ cx<LT>* e2() { return E2; }
+    __device__ LT* dinv1() { return d1; }
+    __device__ cx<LT>* dinv2() { return d2; }
+    __device__ int* perm1() { return p1; }
+    __device__ int* perm2() { return p2; }
+    __device__ double* vbuf() { return buf; }
+    __device__ double* scratch_rhs() { return rhs; }
+    __device__ double* scratch_jac() { return reinterpret_cast<double*>(E2); }
+    // shared-memory bytes of one team (J excluded)
+    static constexpr size_t bytes(int smem_rhs) {
+        return sizeof(LT) * N * N + sizeof(cx<LT>) * N * N + sizeof(LT) * N + sizeof(cx<LT>) * N +
+               2 * sizeof(int) * N + sizeof(double) * N + sizeof(double) * smem_rhs;
+    }
+};
+
+struct RadauParams {
+    double atol, rtol;
+};
+
+template <int N, int TS, class Mech, typename LT, class Store>
+struct Radau {
+    using V = Vec<N, TS>;
+    using TM = Team<TS>;
+    static constexpr int S = V::S;
+
+    const Mech& mech;
+    Store& st;
+    RadauParams prm;
+    double pr;
+    Stats& stats;
+
+    __device__ __forceinline__ void rhs(double t, const V& y, V& f) {
+        mech.template dydt<TS>(t, pr, y, f, st.scratch_rhs());
+        stats.c[ST_RHS]++;
+    }
+
+    __device__ __forceinline__ double err_norm(const V& sc, const V& d) const {
+        double sum = 0.0;
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            if (V::ok(s)) sum += sc[s] * sc[s] * d[s] * d[s];
+        sum = TM::sum(sum);
+        return fmax(sqrt(sum / double(N)), 1e-10);
+    }
+
+    // radau2a.c:256-278; returns info (0 on success)
+    __device__ int decomp(double H) {
+        const double* J = st.jac();
+        LT* E1 = st.e1();
+        cx<LT>* E2 = st.e2();
+        const double g = radau::GAMMA / H, ar = radau::ALPHA / H, ai = radau::BETA / H;
+        const int lane = TM::lane();
+        for (int e = lane; e < N * N; e += TS) {
+            const int i = e % N, j = e / N;
+            const double mj = -J[e];
+            E1[e] = LT(i == j ? mj + g : mj);
+            E2[e] = cx<LT>{LT(i == j ? mj + ar : mj), LT(i == j ? ai : 0.0)};
+        }
+        TM::sync();
+        stats.c[ST_DECOMP]++;
+        int info = lu_real<N, TS, LT>(E1, st.perm1(), st.dinv1());
+        if (info != 0) return info;
+        return lu_cplx<N, TS, LT>(E2, st.perm2(), st.dinv2());
+    }
+
+    // radau2a.c:388-441: Z <- T (E^-1 ((1/h) T^-1 A^-1 Z))
+    __device__ void solve(double H, V& R1, V& R2, V& R3) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const double x1 = R1[s] / H, x2 = R2[s] / H, x3 = R3[s] / H;
+            R1[s] = radau::TIA(0, 0) * x1 + radau::TIA(0, 1) * x2 + radau::TIA(0, 2) * x3;
+            R2[s] = radau::TIA(1, 0) * x1 + radau::TIA(1, 1) * x2 + radau::TIA(1, 2) * x3;
+            R3[s] = radau::TIA(2, 0) * x1 + radau::TIA(2, 1) * x2 + radau::TIA(2, 2) * x3;
+        }
+        double* buf = st.vbuf();
+        permute<N, TS>(R1, st.perm1(), buf);
+        permute<N, TS>(R2, st.perm2(), buf);
+        permute<N, TS>(R3, st.perm2(), buf);
+        lu_solve_pair<N, TS, LT>(st.e1(), st.dinv1(), R1, st.e2(), st.dinv2(), R2, R3);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const double x1 = R1[s], x2 = R2[s], x3 = R3[s];
+            R1[s] = radau::T(0, 0) * x1 + radau::T(0, 1) * x2 + radau::T(0, 2) * x3;
+            R2[s] = radau::T(1, 0) * x1 + radau::T(1, 1) * x2 + radau::T(1, 2) * x3;
+            R3[s] = radau::T(2, 0) * x1 + radau::T(2, 1) * x2 + radau::T(2, 2) * x3;
+        }
+    }
+
+    // E1 x = b with one FP64 refinement step when the factors are single precision.
+    __device__ void solve_e1(double H, V& x) {
+        double* buf = st.vbuf();
+        if (sizeof(LT) == sizeof(double)) {
+            permute<N, TS>(x, st.perm1(), buf);
+            lu_solve_real<N, TS, LT>(st.e1(), st.dinv1(), x);
+            return;
+        }
+        V b = x;
+        permute<N, TS>(x, st.perm1(), buf);
+        lu_solve_real<N, TS, LT>(st.e1(), st.dinv1(), x);
+        // r = b - ((gamma/h) x - J x)
+        const double g = radau::GAMMA / H;
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            if (V::ok(s)) buf[V::idx(s)] = x[s];
+        TM::sync();
+        const double* J = st.jac();
+        V r;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            r[s] = 0.0;
+            if (V::ok(s)) {
+                const int i = V::idx(s);
+                double jx = 0.0;
+                for (int j = 0; j < N; ++j) jx = fma(J[i + N * j], buf[j], jx);
+                r[s] = b[s] - (g * x[s] - jx);
+            }
+        }
+        TM::sync();
+        permute<N, TS>(r, st.perm1(), buf);
+        lu_solve_real<N, TS, LT>(st.e1(), st.dinv1(), r);
+#pragma unroll
+        for (int s = 0; s < S; ++s) x[s] += r[s];
+    }
+
+    // radau2a.c:458-508
+    __device__ double error_estimate(double H, double t, const V& Y, const V& F0, const V& Z1, const V& Z2,
+                                     const V& Z3, const V& sc, bool FirstStep, bool Reject) {
+        const double e1 = radau::E(1) / H, e2 = radau::E(2) / H, e3 = radau::E(3) / H;
+        V F2, TMP;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            F2[s] = e1 * Z1[s] + e2 * Z2[s] + e3 * Z3[s];
+            TMP[s] = radau::E(0) * F0[s] + F2[s];
+        }
+        solve_e1(H, TMP);
+        stats.c[ST_AUX]++;
+        double Err = err_norm(sc, TMP);
+        if (Err >= 1.0 && (FirstStep || Reject)) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) TMP[s] += Y[s];
+            V F1;
+            rhs(t, TMP, F1);
+#pragma unroll
+            for (int s = 0; s < S; ++s) TMP[s] = F1[s] + F2[s];
+            solve_e1(H, TMP);
+            stats.c[ST_AUX]++;
+            Err = err_norm(sc, TMP);
+        }
+        return Err;
+    }
+
+    // radau2a.c:520-736
+    __device__ int integrate(double t_start, double t_end, V& y) {
+        const double ATOL = prm.atol, RTOL = prm.rtol;
+        double Hmin = 0, Hold = 0, Hacc = 0, ErrOld = 0;
+        double H = fmin(5e-7, t_end - t_start);
+        double Hnew;
+        double t = t_start;
+        bool Reject = false, FirstStep = true, SkipJac = false, SkipLU = false;
+        V sc, y0, F0, Z1, Z2, Z3, DZ1, DZ2, DZ3, CONT0, CONT1, CONT2;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            sc[s] = 1.0 / (ATOL + fabs(y[s]) * RTOL);
+            y0[s] = y[s];
+            Z1[s] = Z2[s] = Z3[s] = 0.0;
+            CONT0[s] = CONT1[s] = CONT2[s] = 0.0;
+        }
+        int Nconsecutive = 0, Nsteps = 0;
+        double NewtonRate = pow(2.0, 1.25);
+        while (t + radau::ROUNDOFF < t_end) {
+            if (!Reject) rhs(t, y, F0);
+            if (!SkipLU) {
+                if (!SkipJac) {
+                    mech.template jacob<TS>(t, pr, y, st.jac(), st.scratch_jac());
+                    stats.c[ST_JAC]++;
+                }
+                const int info = decomp(H);
+                if (info != 0) {
+                    Nconsecutive += 1;
+                    if (Nconsecutive >= radau::MAX_CONSECUTIVE_ERRS) return EC_consecutive_steps;
+                    H *= 0.5;
+                    Reject = true;
+                    SkipJac = true;
+                    SkipLU = false;
+                    stats.c[ST_REJECT]++;
+                    continue;
+                }
+                Nconsecutive = 0;
+            }
+            Nsteps += 1;
+            stats.c[ST_STEPS]++;
+            if (Nsteps >= radau::MAX_NO_STEPS) return EC_max_steps_exceeded;
+            if (0.1 * fabs(H) <= fabs(t) * radau::ROUNDOFF) return EC_h_plus_t_equals_h;
+            if (FirstStep) {
+#pragma unroll
+                for (int s = 0; s < S; ++s) Z1[s] = Z2[s] = Z3[s] = 0.0;
+            } else {
+                const double r = H / Hold;
+                const double x1 = 1.0 + radau::C(0) * r, x2 = 1.0 + radau::C(1) * r, x3 = 1.0 + radau::C(2) * r;
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    Z1[s] = CONT0[s] + x1 * (CONT1[s] + x1 * CONT2[s]);
+                    Z2[s] = CONT0[s] + x2 * (CONT1[s] + x2 * CONT2[s]);
+                    Z3[s] = CONT0[s] + x2 * (CONT1[s] + x3 * CONT2[s]);
+                }
+            }
+            bool NewtonDone = false;
+            double NewtonIncrementOld = 0;
+            double Fac = 0.5;
+            int NewtonIter = 0;
+            double Theta = 0;
+            NewtonRate = pow(fmax(NewtonRate, DBL_EPSILON), 0.8);
+            for (; NewtonIter < radau::NEWTON_MAXIT; NewtonIter++) {
+                stats.c[ST_NEWTON]++;
+                // RK_PrepareRHS (radau2a.c:353-383)
+#pragma unroll
+                for (int s = 0; s < S; ++s) { DZ1[s] = Z1[s]; DZ2[s] = Z2[s]; DZ3[s] = Z3[s]; }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    V TMP, F;
+                    const V& Zc = c == 0 ? Z1 : (c == 1 ? Z2 : Z3);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) TMP[s] = y[s] + Zc[s];
+                    rhs(t + radau::C(c) * H, TMP, F);
+                    const double a1 = -H * radau::A(0, c), a2 = -H * radau::A(1, c), a3 = -H * radau::A(2, c);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        DZ1[s] += a1 * F[s];
+                        DZ2[s] += a2 * F[s];
+                        DZ3[s] += a3 * F[s];
+                    }
+                }
+                solve(H, DZ1, DZ2, DZ3);
+                const double d1 = err_norm(sc, DZ1), d2 = err_norm(sc, DZ2), d3 = err_norm(sc, DZ3);
+                const double NewtonIncrement = sqrt((d1 * d1 + d2 * d2 + d3 * d3) / 3.0);
+                Theta = radau::THETA_MIN;
+                if (NewtonIter > 0) {
+                    Theta = NewtonIncrement / NewtonIncrementOld;
+                    if (Theta < 0.99) {
+                        NewtonRate = Theta / (1.0 - Theta);
+                    } else {
+                        break;
+                    }
+                    const double NewtonPredictedErr =
+                        (NewtonIncrement * pow(Theta, double(radau::NEWTON_MAXIT - NewtonIter - 1))) / (1.0 - Theta);
+                    if (NewtonPredictedErr >= radau::NEWTON_TOL) {
+                        const double Qnewton = fmin(10.0, NewtonPredictedErr / radau::NEWTON_TOL);
+                        Fac = 0.8 * pow(Qnewton, -1.0 / double(radau::NEWTON_MAXIT - NewtonIter));
+                        break;
+                    }
+                }
+                NewtonIncrementOld = fmax(NewtonIncrement, radau::ROUNDOFF);
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    Z1[s] -= DZ1[s];
+                    Z2[s] -= DZ2[s];
+                    Z3[s] -= DZ3[s];
+                }
+                NewtonDone = (NewtonRate * NewtonIncrement <= radau::NEWTON_TOL);
+                if (NewtonDone) break;
+                if (NewtonIter == radau::NEWTON_MAXIT - 1) return EC_newton_max_iterations_exceeded;
+            }
+            if (!NewtonDone) {
+                H = Fac * H;
+                Reject = true;
+                SkipJac = true;
+                SkipLU = false;
+                stats.c[ST_REJECT]++;
+                continue;
+            }
+            const double Err = error_estimate(H, t, y, F0, Z1, Z2, Z3, sc, FirstStep, Reject);
+            Fac = pow(Err, (-1.0 / radau::ELO)) * (1.0 + 2 * radau::NEWTON_MAXIT) /
+                  (NewtonIter + 1.0 + 2 * radau::NEWTON_MAXIT);
+            Fac = fmin(radau::FAC_MAX, fmax(radau::FAC_MIN, Fac));
+            Hnew = Fac * H;
+            if (Err < 1.0) {
+                if (!FirstStep) {
+                    double FacGus = radau::FAC_SAFE * (H / Hacc) * pow(Err * Err / ErrOld, -0.25);
+                    FacGus = fmin(radau::FAC_MAX, fmax(radau::FAC_MIN, FacGus));
+                    Fac = fmin(Fac, FacGus);
+                    Hnew = Fac * H;
+                }
+                Hacc = H;
+                ErrOld = fmax(1e-2, Err);
+                FirstStep = false;
+                Hold = H;
+                t += H;
+                stats.c[ST_ACCEPT]++;
+                // y += Z3; interpolant (radau2a.c:283-297); new scale
+                const double c0 = radau::C(0), c1 = radau::C(1), c2 = radau::C(2);
+                const double den = (c2 - c1) * (c1 - c0) * (c0 - c2);
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    y[s] += Z3[s];
+                    CONT0[s] = ((-c2 * c2 * c1 * Z1[s] + Z3[s] * c1 * c0 * c0 + c1 * c1 * c2 * Z1[s] -
+                                 c1 * c1 * c0 * Z3[s] + c2 * c2 * c0 * Z2[s] - Z2[s] * c2 * c0 * c0) /
+                                den) - Z3[s];
+                    CONT1[s] = -(c0 * c0 * (Z3[s] - Z2[s]) + c1 * c1 * (Z1[s] - Z3[s]) + c2 * c2 * (Z2[s] - Z1[s])) / den;
+                    CONT2[s] = (c0 * (Z3[s] - Z2[s]) + c1 * (Z1[s] - Z3[s]) + c2 * (Z2[s] - Z1[s])) / den;
+                    sc[s] = 1.0 / (ATOL + fmax(fabs(y[s]), fabs(y0[s])) * RTOL);
+                    y0[s] = y[s];
+                }
+                Hnew = fmin(fmax(Hnew, Hmin), t_end - t);
+                if (Reject) Hnew = fmin(Hnew, H);
+                Reject = false;
+                if (t + Hnew / radau::Q_MIN - t_end >= 0.0) {
+                    H = t_end - t;
+                } else {
+                    const double Hratio = Hnew / H;
+                    SkipLU = (Theta <= radau::THETA_MIN) && (Hratio >= radau::Q_MIN) && (Hratio <= radau::Q_MAX);
+                    if (!SkipLU) H = Hnew;
+                }
+                SkipJac = NewtonIter == 1 || NewtonRate <= radau::THETA_MIN;
+            } else {
+                if (FirstStep || Reject) {
+                    H = radau::FAC_REJ * H;
+                } else {
+                    H = Hnew;
+                }
+                Reject = true;
+                SkipJac = true;
+                SkipLU = false;
+                stats.c[ST_REJECT]++;
+            }
+        }
+        return EC_success;
+    }
+};
+
+}  // namespace aib

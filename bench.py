@@ -1,0 +1,300 @@
+#!/usr/bin/env python
+"""Throughput benchmark: ODE systems/s per global Delta-t step.
+
+Workload (default): the 53-species / 325-reaction synthetic mechanism, 1,048,576
+initial conditions (half near equilibrium at 800-1200 K, half ignition at
+1400-2400 K, interleaved), Radau IIA at rtol 1e-6 / atol 1e-10, global steps of
+dt = 1e-6 s from t = 0.  A bench step is one global Delta-t step of all
+systems; the timed region runs K consecutive global steps starting from the
+initial conditions (the warm-up runs W steps from the same initial conditions,
+then the state is reset), so the transient after t = 0 is always inside the
+timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--lu fp32|fp64] [--num NUM] [--solver radau2a]
+
+For N > 1 (torchrun, one rank per GPU) every rank integrates its own batch of
+NUM systems (weak scaling, no collective on the data path); the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from accelerint_b200 import mechanism as M  # noqa: E402
+
+DT = 1e-6
+METRIC = "ODE systems/s per Δt step, 53-species Radau: tuned vs plain FP64 at rtol 1e-6"
+UNIT = "system-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--lu", default="fp32", choices=["fp32", "fp64"])
+    p.add_argument("--num", type=int, default=1 << 20)
+    p.add_argument("--solver", default="radau2a")
+    p.add_argument("--seed", type=int, default=2024)
+    p.add_argument("--cpu-sample", type=int, default=0, help="systems in the CPU baseline sample (0: auto)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload(num, seed, rank=0):
+    mech = M.mechanism_53()
+    y, var = M.mixed_stiffness_initial_conditions(mech, num, seed + 7919 * rank)
+    return mech, y, var
+
+
+# ---------------------------------------------------------------- FLOP model
+def flops_per_system(stats, n=54, R=325):
+    """Algorithmic FP64 flops from the device event counters (FMA = 2 flops).
+
+    decomp: (2/3) N^3 real LU + (8/3) N^3 complex LU + N^2 (E1/E2 assembly);
+    newton: 3 RHS (counted separately) + 2 N^2 real + 8 N^2 complex triangular
+            solves + 30 N for transforms/updates + 12 N for the norms;
+    aux (error-estimate solves): 2 N^2 + 8 N;
+    rhs: 14 R + 10 N mass-action evaluation (2 exp counted as 0 flops);
+    jac: 60 R + 4 N^2."""
+    d, nw, rhs, aux, jac = (stats[:, 4], stats[:, 5], stats[:, 6], stats[:, 7], stats[:, 3])
+    f = (d * ((2.0 / 3.0) * n ** 3 + (8.0 / 3.0) * n ** 3 + n * n) +
+         nw * (2 * n * n + 8 * n * n + 42 * n) + aux * (2 * n * n + 8 * n) +
+         rhs * (14 * R + 10 * n) + jac * (60 * R + 4 * n * n))
+    return f
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def measure_fp64_peak(torch):
+    from accelerint_b200 import load_library
+    lib = load_library()
+    import ctypes
+    out = ctypes.c_double(0.0)
+    lib.accelerInt_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    rc = lib.accelerInt_measure_fma_peak(1, ctypes.byref(out))
+    return out.value if rc == 0 else None
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline(args, mech, y, var):
+    """Reference CPU radau2a (oracle/_ref, the reference's own C sources) on a bounded sample."""
+    sys.path.insert(0, ROOT)
+    from oracle import Reference, reference_available, Oracle, oracle_available
+    nthreads = os.cpu_count() or 1
+    sample = args.cpu_sample or 512
+    ys, vs = y[:, :sample].copy(), var[:sample].copy()
+    if reference_available("radau2a", 54):
+        ref = Reference("radau2a", 54)
+        ref.set_mechanism(mech)
+        kind = "reference"
+        t0 = time.time()
+        for k in range(args.steps):
+            ys, codes = ref.integrate(ys, vs, k * DT, (k + 1) * DT, nthreads)
+        el = time.time() - t0
+    elif oracle_available():
+        o = Oracle()
+        kind = "port"
+        t0 = time.time()
+        for k in range(args.steps):
+            ys, codes, _ = o.integrate("radau2a", mech, ys, vs, k * DT, (k + 1) * DT, nthreads=nthreads)
+        el = time.time() - t0
+    else:
+        return None
+    return {"value": sample * args.steps / el, "unit": UNIT, "cores": nthreads, "kind": kind,
+            "sample": f"first {sample} systems (both stiffness halves) x {args.steps} global steps from t=0, "
+                      f"{nthreads} OpenMP threads, {el:.2f} s"}
+
+
+def run_reference_arm(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    mech, y, var = workload(args.num, args.seed)
+    cb = cpu_baseline(args, mech, y, var)
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) and oracle missing"}))
+        return 0
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.num / cb["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "mass-action 53 species / 325 reactions, mixed stiffness, "
+                                                       f"{args.num} ICs, dt=1e-6 s, radau2a rtol 1e-6 atol 1e-10",
+                                            "solver": "radau2a (reference CPU, OpenMP)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import accelerint_b200 as A
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        torch.cuda.set_device(local)
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    mech, y, var = workload(args.num, args.seed, rank)
+    lu = A.LU_FP32 if args.lu == "fp32" else A.LU_FP64
+    integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu)
+    stream = torch.cuda.Stream(device=dev)
+    y0 = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
+    vd = torch.from_numpy(np.ascontiguousarray(var)).to(dev)
+    yd = y0.clone()
+    codes = torch.zeros(args.num, dtype=torch.int32, device=dev)
+    stats = torch.zeros((args.num, A.NSTATS), dtype=torch.int32, device=dev)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # warm-up: W global steps from the initial conditions, then reset
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            integ.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, codes, None, stream)
+        yd.copy_(y0)
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with ClockSampler(dev.index) as clk:
+        barrier()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for k in range(args.steps):
+                integ.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, codes, stats, stream)
+                launches += 1
+            ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    t_max = ms
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    nfail = int((codes != 0).sum().item())
+    st = stats.cpu().numpy().astype(np.float64)
+    flops = float(flops_per_system(st).sum())
+    value = ws * args.num * args.steps / (t_max / 1000.0)
+    peak = measure_fp64_peak(torch) if rank == 0 else None
+    achieved = flops / (ms / 1000.0) / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None, "traffic": None,
+                "note": "algorithmic FP64 flops from device event counters per system "
+                        "(decomp, Newton, RHS, error solves, Jacobians) over the kernel time; "
+                        "peak = FP64 FMA microbenchmark measured in this run"}
+    # e2e: the C-ABI host path (accelerInt_integrate_status) with host buffers, copies inside the timing
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.time()
+        yh = y.copy()
+        for k in range(args.steps):
+            yh, c, rc = integ.integrate(k * DT, (k + 1) * DT, DT, yh, var)
+        el = time.time() - t0
+        nb = args.num * (mech.n_state + 1) * 8
+        e2e = {"value": ws * args.num * args.steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": args.num * mech.n_state * 8 + args.num * 4}
+    line = None
+    if rank == 0:
+        cb = None if args.no_cpu_baseline else cpu_baseline(args, mech, y, var)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"mass-action 53 species / 325 reactions, mixed stiffness, {args.num} ICs "
+                                       f"per GPU, global steps of dt=1e-6 s from t=0, {args.solver} rtol 1e-6 "
+                                       f"atol 1e-10, LU {args.lu}, persistent work-queue team kernel",
+                           "l2": "inputs (y: 432 MB per GPU) larger than L2; no flush",
+                           "failed_systems": nfail},
+                "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cb}
+        print(json.dumps(line))
+    integ.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

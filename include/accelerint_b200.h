@@ -1,0 +1,127 @@
+/*
+ * accelerint_b200 -- batched stiff-ODE integration on one NVIDIA B200 (sm_100a),
+ * a drop-in for accelerInt's GPU library interface.
+ *
+ * The three legacy entry points keep the reference's signatures and meaning:
+ *
+ *   accelerInt_initialize   generic/solver_interface.cuh:35  (solver_interface.cu:88-147)
+ *   accelerInt_integrate    generic/solver_interface.cuh:49  (solver_interface.cu:161-211)
+ *   accelerInt_cleanup      generic/solver_interface.cuh:55  (solver_interface.cu:217-225)
+ *
+ * Layout (unchanged from the reference, examples/main.dox:70-82): y_host is
+ * column-major with the IVP index fastest, y_host[i * NUM + ivp], overwritten
+ * with the state at t_end; var_host[ivp] is the per-system parameter
+ * (pressure in Pa for the mass-action mechanism, mu for van der Pol).
+ *
+ * Differences from the reference, by design:
+ *   - no process exit on a failed system or CUDA error: the legacy void calls
+ *     record the status (accelerInt_last_status) and per-system codes
+ *     (accelerInt_get_codes, the reference's EC_* values 0..4);
+ *   - no cudaDeviceReset in initialize/cleanup (it destroys other users'
+ *     contexts in the same process);
+ *   - solver, mechanism, tolerances and precision are chosen at run time
+ *     through the extension calls below (the reference fixes them at compile
+ *     time: generic/solver_props.h:9-16, SConstruct:181-185);
+ *   - the global-step loop runs t_start -> t_end in steps of stepsize measured
+ *     from t_start (the reference's GPU loop measures from 0 and seeds t_next
+ *     from the end_time macro, solver_interface.cu:166,209).
+ *
+ * Thread safety: one integrator instance per process, as in the reference
+ * (process-global state, solver_interface.cu:18-28).
+ */
+#ifndef ACCELERINT_B200_H
+#define ACCELERINT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- legacy interface (generic/solver_interface.cuh) ---- */
+
+/* Select the device (< 0 means 0) and size device memory for up to NUM systems
+ * per batch.  Replaces solver_interface.cuh:35. */
+void accelerInt_initialize(int NUM, int device);
+
+/* Integrate NUM systems from t_start to t_end in global steps of stepsize
+ * (stepsize < 0: one step of t_end - t_start).  Synchronous: y_host holds the
+ * result when the call returns.  Replaces solver_interface.cuh:49-50. */
+void accelerInt_integrate(const int NUM, const double t_start, const double t_end,
+                          const double stepsize, double* y_host, const double* var_host);
+
+/* Release device memory.  Replaces solver_interface.cuh:55. */
+void accelerInt_cleanup(void);
+
+/* ---- extensions (no counterpart in the reference's interface) ---- */
+
+/* status codes returned by the extension calls */
+#define ACCELERINT_OK 0
+#define ACCELERINT_ERR_ARGUMENT -1      /* invalid argument */
+#define ACCELERINT_ERR_CUDA -2          /* a CUDA call failed */
+#define ACCELERINT_ERR_STATE -3         /* not initialised / no mechanism */
+#define ACCELERINT_ERR_UNSUPPORTED -4   /* (solver, mechanism size, precision) not built */
+#define ACCELERINT_ERR_SYSTEMS -5       /* at least one system returned a nonzero EC_* code */
+
+/* solvers (generic/solver_props.h:9-16 selects one of these at compile time) */
+#define ACCELERINT_RADAU2A 0
+#define ACCELERINT_EXPRB43 1
+#define ACCELERINT_EXP4 2
+#define ACCELERINT_RKC 3
+
+/* precision of the Radau simplified-Newton matrices E1/E2 */
+#define ACCELERINT_LU_FP64 0
+#define ACCELERINT_LU_FP32 1   /* factor + solve in FP32; residuals, error estimate, control in FP64 */
+
+/* Synthetic constant-pressure mass-action mechanism (plain tables; see
+ * accelerint_b200/mechanism.py for the model).  Stands in for the pyJac
+ * dydt/eval_jacob slot (examples/van_der_pol/dydt.h, jacob.h). */
+typedef struct {
+    int n_species;          /* K; state length N = K + 1 (T, Y_1..Y_K) */
+    int n_reactions;        /* R */
+    const double* mw;       /* [K] kg/mol */
+    const double* cp;       /* [K] J/mol/K */
+    const double* h_form;   /* [K] J/mol at 298.15 K */
+    const double* s_ref;    /* [K] J/mol/K at 298.15 K */
+    const int* reac;        /* [R*2] reactant species, -1 = empty slot */
+    const int* prod;        /* [R*2] product species, -1 = empty slot */
+    const double* log_a;    /* [R] ln A, (cm^3/mol)^(order-1)/s */
+    const double* beta;     /* [R] temperature exponent */
+    const double* ta;       /* [R] activation temperature Ea/R [K] */
+} accelerInt_mass_action;
+
+int accelerInt_set_solver(int solver);
+int accelerInt_set_mechanism_van_der_pol(void);
+int accelerInt_set_mechanism_mass_action(const accelerInt_mass_action* mech);
+int accelerInt_set_tolerances(double atol, double rtol);   /* defaults 1e-10 / 1e-6 */
+int accelerInt_set_lu_precision(int precision);             /* ACCELERINT_LU_FP64 (default) */
+
+/* Like accelerInt_integrate, returning ACCELERINT_OK, ACCELERINT_ERR_SYSTEMS or an error. */
+int accelerInt_integrate_status(int NUM, double t_start, double t_end, double stepsize,
+                                double* y_host, const double* var_host);
+
+/* Device-resident form: y_dev[i * NUM + ivp] and var_dev[NUM] are device
+ * pointers; codes_dev[NUM] (optional, may be NULL) receives the EC_* code of
+ * each system; stats_dev (optional) receives ACCELERINT_NSTATS int counters per
+ * system, stats_dev[ivp * ACCELERINT_NSTATS + k], added to what the array holds
+ * (zero it before the first call).  Asynchronous on `stream`
+ * (a cudaStream_t, NULL = the legacy default stream). */
+#define ACCELERINT_NSTATS 8   /* steps, accept, reject, jac, decomp, newton, rhs, errsolve/krylov */
+int accelerInt_integrate_device(int NUM, double t_start, double t_end, double stepsize,
+                                double* y_dev, const double* var_dev, int* codes_dev,
+                                int* stats_dev, void* stream);
+
+int accelerInt_last_status(void);
+/* Copies the EC_* codes of the last accelerInt_integrate* call (host pointer, NUM entries). */
+int accelerInt_get_codes(int* codes_host, int NUM);
+/* Poles and residues of the (10,10) rational approximant in use (exp methods). */
+int accelerInt_get_poles(double* poles_re, double* poles_im, double* res_re, double* res_im);
+const char* accelerInt_version(void);
+
+/* Diagnostic: measured FMA throughput of the current device in TFLOP/s (FMA = 2
+ * flops), fp64 != 0 for double precision, else single.  Used as the roofline
+ * denominator for the FP64/FP32 integrator kernels. */
+int accelerInt_measure_fma_peak(int fp64, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
