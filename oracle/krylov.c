@@ -258,10 +258,13 @@ int or_exprb43(const or_config* c, const or_mech* mech, double t_start, double t
     double beta = 0;
     double temp[OR_NMAX], f_temp[OR_NMAX], y1[OR_NMAX], fy[OR_NMAX], gy[OR_NMAX];
     double A[OR_NMAX * OR_NMAX] = {0.0};
-    static const double zero_init = 0.0;
     double Hm[OR_STRIDE_MAX * OR_STRIDE_MAX];
-    for (int i = 0; i < stride * stride; ++i) Hm[i] = zero_init;
+    for (int i = 0; i < OR_STRIDE_MAX * OR_STRIDE_MAX; ++i) Hm[i] = 0.0;
+    /* zero-initialised: arnoldi() reads basis column j after a happy breakdown
+     * without writing it (arnoldi.h:118); the reference leaves it uninitialised */
     double Vm[OR_NMAX * OR_STRIDE_MAX], phiHm[OR_STRIDE_MAX * OR_STRIDE_MAX];
+    for (int i = 0; i < OR_NMAX * OR_STRIDE_MAX; ++i) Vm[i] = 0.0;
+    for (int i = 0; i < OR_STRIDE_MAX * OR_STRIDE_MAX; ++i) phiHm[i] = 0.0;
     double err = 0.0;
     double savedActions[OR_NMAX * 5];
     (void)P;
@@ -404,8 +407,10 @@ int or_exp4(const or_config* c, const or_mech* mech, double t_start, double t_en
     double A[OR_NMAX * OR_NMAX] = {0.0};
     double temp[OR_NMAX], f_temp[OR_NMAX], y1[OR_NMAX];
     double Hm[OR_STRIDE_MAX * OR_STRIDE_MAX];
-    for (int i = 0; i < stride * stride; ++i) Hm[i] = 0.0;
+    for (int i = 0; i < OR_STRIDE_MAX * OR_STRIDE_MAX; ++i) Hm[i] = 0.0;
     double Vm[OR_NMAX * OR_STRIDE_MAX], phiHm[OR_STRIDE_MAX * OR_STRIDE_MAX];
+    for (int i = 0; i < OR_NMAX * OR_STRIDE_MAX; ++i) Vm[i] = 0.0;   /* see or_exprb43 */
+    for (int i = 0; i < OR_STRIDE_MAX * OR_STRIDE_MAX; ++i) phiHm[i] = 0.0;
     double err = 0.0;
     double k1[OR_NMAX], k2[OR_NMAX], k3[OR_NMAX], k4[OR_NMAX], k5[OR_NMAX], k6[OR_NMAX], k7[OR_NMAX];
     while ((t < t_end) && (t + h > t)) {
