@@ -11,5 +11,5 @@ ivp]``).  There is no CPU fallback: if the library is missing, importing
 from .mechanism import (MassAction, VanDerPol, mechanism_13, mechanism_53,  # noqa: F401
                         mass_action_initial_conditions, mixed_stiffness_initial_conditions,
                         synthetic_mechanism, vdp_initial_conditions)
-from ._lib import (ACCELERINT_ERR_SYSTEMS, ACCELERINT_OK, EXPORTED_SYMBOLS, LU_FP32, LU_FP64,  # noqa: F401
+from ._lib import (ACCELERINT_ERR_SYSTEMS, ACCELERINT_OK, EXPORTED_SYMBOLS, LU_FP32, LU_FP32_ALL, LU_FP64,  # noqa: F401
                    NSTATS, SOLVERS, Integrator, library_path, load_library)

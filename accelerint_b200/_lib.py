@@ -17,7 +17,7 @@ ACCELERINT_ERR_STATE = -3
 ACCELERINT_ERR_UNSUPPORTED = -4
 ACCELERINT_ERR_SYSTEMS = -5
 SOLVERS = {"radau2a": 0, "exprb43": 1, "exp4": 2, "rkc": 3}
-LU_FP64, LU_FP32 = 0, 1
+LU_FP64, LU_FP32, LU_FP32_ALL = 0, 1, 2
 NSTATS = 8
 STAT_NAMES = ["steps", "accept", "reject", "jac", "decomp", "newton", "rhs", "aux"]
 

@@ -117,6 +117,7 @@ int upload_mass_action() {
     t.sp_ent = static_cast<const int*>(put(m.sp_ent.data(), m.sp_ent.size() * sizeof(int)));
     CK(cudaGetLastError());
     g.dev_tb = t;
+    CK(cudaMemcpyToSymbol(c_ma, &t, sizeof(t)));
     return ACCELERINT_OK;
 }
 
@@ -132,12 +133,12 @@ template <class K> int persistent_grid(K kernel, int block, size_t smem, int num
     return ACCELERINT_OK;
 }
 
-template <int SK, class Mech, int TS, typename LT>
+template <int SK, class Mech, int TS, typename LT, typename L1 = LT>
 int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
     constexpr int N = Mech::N;
-    const int block = 32, tpb = block / TS;
+    const int block = TS >= 32 ? TS : 32, tpb = block / TS;
     const size_t smem = size_t(lay.total) * tpb;
-    auto kern = team_kernel<SK, Mech, TS, LT>;
+    auto kern = team_kernel<SK, Mech, TS, LT, L1>;
     int grid = 0;
     int rc = persistent_grid(kern, block, smem, a.num, tpb, &grid);
     if (rc) return rc;
@@ -154,13 +155,16 @@ template <int K, int TS>
 int launch_mass_action(BatchArgs a, cudaStream_t s) {
     using M = MassAction<K>;
     M mech;
-    mech.tb = g.dev_tb;
     const int R = g.mt.R;
     constexpr int N = M::N;
     if (g.solver == ACCELERINT_RADAU2A) {
         if (g.lu == ACCELERINT_LU_FP32) {
-            TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R));
-            return launch_team<SK_RADAU, M, TS, float>(a, mech, lay, s);
+            TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 8);
+            return launch_team<SK_RADAU, M, TS, float, double>(a, mech, lay, s);
+        }
+        if (g.lu == ACCELERINT_LU_FP32_ALL) {
+            TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 4);
+            return launch_team<SK_RADAU, M, TS, float, float>(a, mech, lay, s);
         }
         TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
         return launch_team<SK_RADAU, M, TS, double>(a, mech, lay, s);
@@ -190,8 +194,8 @@ int launch(BatchArgs a, cudaStream_t s) {
     if (a.num <= 0) return ACCELERINT_OK;
     if (g.mech_kind == 0) return launch_vdp(a, s);
     switch (g.mt.K) {
-        case 13: return launch_mass_action<13, 16>(a, s);
-        case 53: return launch_mass_action<53, 32>(a, s);
+        case 13: return launch_mass_action<13, 32>(a, s);
+        case 53: return launch_mass_action<53, 64>(a, s);
         default: return ACCELERINT_ERR_UNSUPPORTED;
     }
 }
@@ -364,7 +368,8 @@ int accelerInt_set_tolerances(double atol, double rtol) {
 }
 
 int accelerInt_set_lu_precision(int precision) {
-    if (precision != ACCELERINT_LU_FP64 && precision != ACCELERINT_LU_FP32) return ACCELERINT_ERR_ARGUMENT;
+    if (precision != ACCELERINT_LU_FP64 && precision != ACCELERINT_LU_FP32 && precision != ACCELERINT_LU_FP32_ALL)
+        return ACCELERINT_ERR_ARGUMENT;
     g.lu = precision;
     return ACCELERINT_OK;
 }

@@ -67,52 +67,80 @@ template <typename T> __device__ __forceinline__ cx<T> cdiv(cx<T> a, cx<T> b) {
 }
 
 // ------------------------------------------------------------------ teams
-// A team of TS consecutive lanes of one warp integrates one system.  TS = 1 is
-// a thread per system (everything in registers); TS = 16 or 32 share the
-// system's matrices in shared memory.  Control decisions must be identical on
-// every lane of a team, so every reduction ends with a broadcast of one lane's
-// value (a butterfly alone can leave lanes with differently rounded sums).
+// A team of TS threads integrates one system.  TS = 1 is a thread per system
+// (everything in registers); TS = 2..16 are lane groups inside one warp; TS =
+// 32 or 64 is a whole thread block (one system per block) whose threads own
+// one state element each and share the system's matrices in shared memory.
+// Control decisions must be identical on every thread of a team, so every
+// reduction ends with a broadcast of one value (a butterfly alone can leave
+// lanes with differently rounded sums).
 template <int TS> struct Team {
-    static_assert(TS == 1 || TS == 2 || TS == 4 || TS == 8 || TS == 16 || TS == 32, "team size");
+    static_assert(TS == 1 || TS == 2 || TS == 4 || TS == 8 || TS == 16 || TS == 32 || TS == 64, "team size");
     static constexpr int size = TS;
+    static constexpr bool block = TS >= 32;        // one team per thread block
+    static constexpr int W = TS >= 32 ? TS / 32 : 1;
+    static constexpr int WS = TS < 32 ? TS : 32;   // width of the warp-level part
     __device__ __forceinline__ static int lane() { return TS == 1 ? 0 : int(threadIdx.x & (TS - 1)); }
+    __device__ __forceinline__ static int warp() { return block ? int(threadIdx.x >> 5) : 0; }
     __device__ __forceinline__ static unsigned mask() {
-        if (TS == 32) return 0xffffffffu;
+        if (TS >= 32) return 0xffffffffu;
         if (TS == 1) return 1u << (threadIdx.x & 31);
         const unsigned base = (threadIdx.x & 31) & ~unsigned(TS - 1);
         return ((1u << TS) - 1u) << base;
     }
     __device__ __forceinline__ static void sync() {
-        if (TS > 1) __syncwarp(mask());
+        if (TS > 32) __syncthreads();
+        else if (TS > 1) __syncwarp(mask());
+    }
+    __device__ __forceinline__ static double wsum(double v) {
+#pragma unroll
+        for (int o = WS / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask(), v, o, WS);
+        return __shfl_sync(mask(), v, 0, WS);
     }
     __device__ __forceinline__ static double bcast(double v, int src) {
         if (TS == 1) return v;
-        return __shfl_sync(mask(), v, src, TS);
+        if (TS <= 32) return __shfl_sync(mask(), v, src, TS);
+        __shared__ double b;
+        __syncthreads();
+        if (lane() == src) b = v;
+        __syncthreads();
+        return b;
     }
     __device__ __forceinline__ static int bcast(int v, int src) {
         if (TS == 1) return v;
-        return __shfl_sync(mask(), v, src, TS);
+        if (TS <= 32) return __shfl_sync(mask(), v, src, TS);
+        __shared__ int b;
+        __syncthreads();
+        if (lane() == src) b = v;
+        __syncthreads();
+        return b;
     }
     __device__ __forceinline__ static double sum(double v) {
         if (TS == 1) return v;
+        v = wsum(v);
+        if (TS <= 32) return v;
+        __shared__ double red[W];
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) red[warp()] = v;
+        __syncthreads();
+        double s = red[0];
 #pragma unroll
-        for (int o = TS / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask(), v, o, TS);
-        return __shfl_sync(mask(), v, 0, TS);
+        for (int w = 1; w < W; ++w) s += red[w];
+        return s;
     }
-    __device__ __forceinline__ static double max(double v) {
-        if (TS == 1) return v;
-#pragma unroll
-        for (int o = TS / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask(), v, o, TS));
-        return __shfl_sync(mask(), v, 0, TS);
-    }
-    // argmax of v with ties to the smallest index; returns the index on every lane
+    // argmax of v with ties to the smallest index (warp-level teams only); an
+    // index of INT_MAX marks "no candidate on this lane"; NaN loses to a number
     __device__ __forceinline__ static int argmax(double v, int idx) {
+        static_assert(TS <= 32, "warp-level argmax");
         if (TS == 1) return idx;
 #pragma unroll
         for (int o = TS / 2; o > 0; o >>= 1) {
             double ov = __shfl_xor_sync(mask(), v, o, TS);
             int oi = __shfl_xor_sync(mask(), idx, o, TS);
-            if (ov > v || (ov == v && oi < idx) || (v != v && ov == ov)) { v = ov; idx = oi; }
+            if (oi != 0x7fffffff && (idx == 0x7fffffff || ov > v || (ov == v && oi < idx) || (v != v && ov == ov))) {
+                v = ov;
+                idx = oi;
+            }
         }
         return __shfl_sync(mask(), idx, 0, TS);
     }

@@ -95,21 +95,25 @@ __global__ void __launch_bounds__(128) tps_kernel(BatchArgs a, Mech mech)
 // ------------------------------------------------------------- team per system
 // Shared-memory layout of one team (bytes, 16-byte aligned pieces).
 struct TeamLayout {
-    int e1, e2, d1, d2, p1, p2, buf, rhs, total;
+    int e1, e2, d1, d2, p1, p2, buf, rhs, inf, total;
     __host__ __device__ static int al(int b) { return (b + 15) & ~15; }
-    __host__ __device__ static TeamLayout radau(int N, int lt_bytes, int rhs_doubles, int jac_doubles) {
+    // lt_bytes: element size of E2's real type; l1_bytes: of E1
+    __host__ __device__ static TeamLayout radau(int N, int lt_bytes, int rhs_doubles, int jac_doubles,
+                                                int l1_bytes = 0) {
         TeamLayout L;
         int o = 0;
-        L.e1 = o; o += al(N * N * lt_bytes);
+        if (l1_bytes == 0) l1_bytes = lt_bytes;
+        L.e1 = o; o += al(N * N * l1_bytes);
         L.e2 = o;
         const int e2b = N * N * 2 * lt_bytes, jb = jac_doubles * 8;
         o += al(e2b > jb ? e2b : jb);
-        L.d1 = o; o += al(N * lt_bytes);
+        L.d1 = o; o += al(N * l1_bytes);
         L.d2 = o; o += al(N * 2 * lt_bytes);
         L.p1 = o; o += al(N * 4);
         L.p2 = o; o += al(N * 4);
-        L.buf = o; o += al(N * 8);
+        L.buf = o; o += al(3 * N * 8);
         L.rhs = o; o += al(rhs_doubles * 8);
+        L.inf = o; o += al(2 * 4);
         L.total = o;
         return L;
     }
@@ -122,8 +126,8 @@ struct TeamLayout {
     }
 };
 
-template <int SK, class Mech, int TS, typename LT>
-__global__ void __launch_bounds__(32) team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
+template <int SK, class Mech, int TS, typename LT, typename L1 = LT>
+__global__ void __launch_bounds__(TS >= 32 ? TS : 32) team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
 {
     constexpr int N = Mech::N;
     using TM = Team<TS>;
@@ -148,17 +152,18 @@ __global__ void __launch_bounds__(32) team_kernel(BatchArgs a, Mech mech, TeamLa
         int code = EC_success;
         StepLoop L(a.t_start, a.t_end, a.step);
         if constexpr (SK == SK_RADAU) {
-            RadauTeamStore<N, LT> store;
+            RadauTeamStore<N, LT, L1> store;
             store.J = a.jac + size_t(gteam) * N * N;
-            store.E1 = reinterpret_cast<LT*>(base + lay.e1);
+            store.E1 = reinterpret_cast<L1*>(base + lay.e1);
             store.E2 = reinterpret_cast<cx<LT>*>(base + lay.e2);
-            store.d1 = reinterpret_cast<LT*>(base + lay.d1);
+            store.d1 = reinterpret_cast<L1*>(base + lay.d1);
             store.d2 = reinterpret_cast<cx<LT>*>(base + lay.d2);
             store.p1 = reinterpret_cast<int*>(base + lay.p1);
             store.p2 = reinterpret_cast<int*>(base + lay.p2);
             store.buf = reinterpret_cast<double*>(base + lay.buf);
             store.rhs = reinterpret_cast<double*>(base + lay.rhs);
-            Radau<N, TS, Mech, LT, RadauTeamStore<N, LT>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
+            store.inf = reinterpret_cast<int*>(base + lay.inf);
+            Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
             while (L.more() && code == EC_success) {
                 code = rad.integrate(L.t, L.t_next, y);
                 L.advance();

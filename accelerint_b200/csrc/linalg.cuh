@@ -31,10 +31,10 @@ __device__ int lu_real(T* A, int* perm, T* dinv)
 #pragma unroll 1
     for (int k = 0; k < N; ++k) {
         double best = -1.0;
-        int bi = N;
+        int bi = 0x7fffffff;   // no candidate on this lane
         for (int i = k + lane; i < N; i += TS) {
             double a = fabs(double(A[i + k * N]));
-            if (a > best || (best != best)) { best = a; bi = i; }
+            if (!(a <= best)) { best = a; bi = i; }   // NaN-safe: a row is always taken
         }
         const int p = TM::argmax(best, bi);
         const T piv = A[p + k * N];
@@ -105,10 +105,10 @@ __device__ int lu_cplx(cx<T>* A, int* perm, cx<T>* dinv)
 #pragma unroll 1
     for (int k = 0; k < N; ++k) {
         double best = -1.0;
-        int bi = N;
+        int bi = 0x7fffffff;   // no candidate on this lane
         for (int i = k + lane; i < N; i += TS) {
             double a = double(cabs1(A[i + k * N]));
-            if (a > best || (best != best)) { best = a; bi = i; }
+            if (!(a <= best)) { best = a; bi = i; }   // NaN-safe: a row is always taken
         }
         const int p = TM::argmax(best, bi);
         const cx<T> piv = A[p + k * N];

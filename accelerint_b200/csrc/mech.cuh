@@ -60,6 +60,215 @@ constexpr double T_REF = 298.15;
 // iterates of an over-long step with unphysical temperatures stay finite.
 constexpr double T_FLOOR = 100.0;
 
+
+// Tables of the mechanism in use (pointers into global memory; one mechanism
+// per process, as the reference compiles one into its library).
+__constant__ MassActionTables c_ma;
+
+// One state element per thread of a block team of TS threads (TS > K):
+// thread t owns y_t (t = 0: temperature, t = 1 + k: mass fraction of k).
+// Shared scratch sm: ys[N], C[K], h[K], grt[K], then per reaction q (dydt) or
+// q, dqdT, dH, dqdC[4] (jacob).  Out of line: one copy serves every call site.
+template <int K> struct MaPrep {
+    double T, S, c0, cpm, logT, log_catm;
+};
+
+template <int K, int TS>
+__device__ __forceinline__ MaPrep<K> ma_prepare(double P, double yi, double* ys, double* C, double* h, double* grt)
+{
+    constexpr int N = K + 1;
+    using TM = Team<TS>;
+    const int t = TM::lane();
+    const MassActionTables& tb = c_ma;
+    if (t < N) ys[t] = yi;
+    TM::sync();
+    MaPrep<K> p;
+    p.T = fmax(ys[0], T_FLOOR);
+    double S = 0.0, cpm = 0.0;
+    if (t < K) {
+        const double yk = ys[1 + t] * __ldg(tb.inv_mw + t);
+        S = yk;
+        cpm = yk * __ldg(tb.cp + t);
+    }
+    p.S = TM::sum(S);
+    p.cpm = TM::sum(cpm);
+    p.c0 = 1e-6 * P / (R_U * p.T);
+    p.logT = log(p.T);
+    p.log_catm = log(1e-6 * P_ATM / (R_U * p.T));
+    if (t < K) {
+        const double lnt = log(p.T / T_REF);
+        C[t] = (p.c0 / p.S) * (ys[1 + t] * __ldg(tb.inv_mw + t));
+        const double cpk = __ldg(tb.cp + t);
+        const double hk = __ldg(tb.h_form + t) + cpk * (p.T - T_REF);
+        h[t] = hk;
+        grt[t] = hk / (R_U * p.T) - (__ldg(tb.s_ref + t) + cpk * lnt) * (1.0 / R_U);
+    }
+    TM::sync();
+    return p;
+}
+
+template <int K>
+__device__ __forceinline__ void ma_rates(int r, const MaPrep<K>& p, const double* grt, int4 sp, double& kf,
+                                         double& kr, int& nre, int& npd)
+{
+    const MassActionTables& tb = c_ma;
+    double g = grt[sp.z] - grt[sp.x];
+    nre = 1;
+    npd = 1;
+    if (sp.y >= 0) { g -= grt[sp.y]; nre = 2; }
+    if (sp.w >= 0) { g += grt[sp.w]; npd = 2; }
+    const double lkf = __ldg(tb.log_a + r) + __ldg(tb.beta + r) * p.logT - __ldg(tb.ta + r) / p.T;
+    kf = exp(lkf);
+    kr = exp(lkf + g - double(npd - nre) * p.log_catm);
+}
+
+// f(y)_t for the calling thread's element t.
+template <int K, int TS>
+__device__ __noinline__ double ma_dydt(double P, double yi, double* sm)
+{
+    constexpr int N = K + 1;
+    using TM = Team<TS>;
+    const int t = TM::lane();
+    const MassActionTables& tb = c_ma;
+    double* ys = sm;
+    double* C = ys + N;
+    double* h = C + K;
+    double* grt = h + K;
+    double* q = grt + K;
+    const int R = tb.R;
+    const MaPrep<K> p = ma_prepare<K, TS>(P, yi, ys, C, h, grt);
+    for (int r = t; r < R; r += TS) {
+        const int4 sp = __ldg(tb.rsp + r);
+        double kf, kr;
+        int nre, npd;
+        ma_rates<K>(r, p, grt, sp, kf, kr, nre, npd);
+        double fwd = kf * C[sp.x];
+        if (nre == 2) fwd *= C[sp.y];
+        double rev = kr * C[sp.z];
+        if (npd == 2) rev *= C[sp.w];
+        q[r] = fwd - rev;
+    }
+    TM::sync();
+    double Qp = 0.0, out = 0.0;
+    if (t >= 1 && t < N) {
+        const int k = t - 1;
+        double w = 0.0;
+        const int e1 = __ldg(tb.sp_ptr + k + 1);
+        for (int e = __ldg(tb.sp_ptr + k); e < e1; ++e) {
+            const int ent = __ldg(tb.sp_ent + e);
+            const double qr = q[ent >> 2];
+            w = (ent & 3) < 2 ? w - qr : w + qr;
+        }
+        Qp = h[k] * w;
+        out = __ldg(tb.mw + k) * (p.S / p.c0) * w;
+    }
+    const double Q = TM::sum(Qp);
+    if (t == 0) out = -p.S * Q / (p.c0 * p.cpm);
+    TM::sync();
+    return out;
+}
+
+// Analytic Jacobian into column-major J[N*N] (global memory); thread t writes row t.
+template <int K, int TS>
+__device__ __noinline__ void ma_jacob(double P, double yi, double* J, double* sm)
+{
+    constexpr int N = K + 1;
+    using TM = Team<TS>;
+    const int t = TM::lane();
+    const MassActionTables& tb = c_ma;
+    const int R = tb.R;
+    double* ys = sm;
+    double* C = ys + N;
+    double* h = C + K;
+    double* grt = h + K;
+    double* q = grt + K;
+    double* dqT = q + R;
+    double* dH = dqT + R;
+    double* dqC = dH + R;   // [R][4]
+    const MaPrep<K> p = ma_prepare<K, TS>(P, yi, ys, C, h, grt);
+    for (int r = t; r < R; r += TS) {
+        const int4 sp = __ldg(tb.rsp + r);
+        double kf, kr;
+        int nre, npd;
+        ma_rates<K>(r, p, grt, sp, kf, kr, nre, npd);
+        const double c_r0 = C[sp.x], c_r1 = nre == 2 ? C[sp.y] : 1.0;
+        const double c_p0 = C[sp.z], c_p1 = npd == 2 ? C[sp.w] : 1.0;
+        const double fwd = kf * c_r0 * c_r1;
+        const double rev = kr * c_p0 * c_p1;
+        double dh = h[sp.z] - h[sp.x];
+        if (npd == 2) dh += h[sp.w];
+        if (nre == 2) dh -= h[sp.y];
+        const double dlkf = (__ldg(tb.beta + r) + __ldg(tb.ta + r) / p.T) / p.T;
+        const double dlkr = dlkf - dh / (R_U * p.T * p.T) + double(npd - nre) / p.T;
+        q[r] = fwd - rev;
+        dqT[r] = fwd * dlkf - rev * dlkr - (nre * fwd - npd * rev) / p.T;
+        dH[r] = dh;
+        dqC[4 * r + 0] = kf * c_r1;
+        dqC[4 * r + 1] = nre == 2 ? kf * c_r0 : 0.0;
+        dqC[4 * r + 2] = -kr * c_p1;
+        dqC[4 * r + 3] = npd == 2 ? -kr * c_p0 : 0.0;
+    }
+    TM::sync();
+    const double inv_c0 = 1.0 / p.c0;
+    double hgp = 0.0, Qp = 0.0, dQTp = 0.0;
+    if (t >= 1 && t < N) {
+        const int k = t - 1;
+        double w = 0.0, wT = 0.0, g = 0.0;
+        const int e0 = __ldg(tb.sp_ptr + k), e1 = __ldg(tb.sp_ptr + k + 1);
+        for (int e = e0; e < e1; ++e) {
+            const int ent = __ldg(tb.sp_ent + e);
+            const int r = ent >> 2;
+            const double nu = (ent & 3) < 2 ? -1.0 : 1.0;
+            const int4 sp = __ldg(tb.rsp + r);
+            w += nu * q[r];
+            wT += nu * dqT[r];
+            double gr = dqC[4 * r + 0] * C[sp.x] + dqC[4 * r + 2] * C[sp.z];
+            if (sp.y >= 0) gr += dqC[4 * r + 1] * C[sp.y];
+            if (sp.w >= 0) gr += dqC[4 * r + 3] * C[sp.w];
+            g += nu * gr * inv_c0;
+        }
+        hgp = h[k] * g;
+        Qp = h[k] * w;
+        dQTp = __ldg(tb.cp + k) * w + h[k] * wT;
+        // dense part of row t, then the sparse G entries of the same row
+        const double a = w * inv_c0 - g;
+        const double wmk = __ldg(tb.mw + k);
+        for (int j = 0; j < K; ++j) J[t + N * (1 + j)] = wmk * __ldg(tb.inv_mw + j) * a;
+        J[t] = (wmk * p.S * inv_c0) * (wT + w / p.T);
+        for (int e = e0; e < e1; ++e) {
+            const int ent = __ldg(tb.sp_ent + e);
+            const int r = ent >> 2;
+            const double nu = (ent & 3) < 2 ? -1.0 : 1.0;
+            const int4 sp = __ldg(tb.rsp + r);
+            J[t + N * (1 + sp.x)] += wmk * __ldg(tb.inv_mw + sp.x) * nu * dqC[4 * r + 0];
+            if (sp.y >= 0) J[t + N * (1 + sp.y)] += wmk * __ldg(tb.inv_mw + sp.y) * nu * dqC[4 * r + 1];
+            J[t + N * (1 + sp.z)] += wmk * __ldg(tb.inv_mw + sp.z) * nu * dqC[4 * r + 2];
+            if (sp.w >= 0) J[t + N * (1 + sp.w)] += wmk * __ldg(tb.inv_mw + sp.w) * nu * dqC[4 * r + 3];
+        }
+    }
+    const double hg = TM::sum(hgp);
+    const double Q = TM::sum(Qp);
+    const double dQT = TM::sum(dQTp);
+    const double f = -1.0 / (p.c0 * p.cpm);
+    if (t < K) {
+        // temperature row, column 1 + t: sum_r dH_r dq_r/dC_t over the reactions of species t
+        double hG = 0.0;
+        const int e1 = __ldg(tb.sp_ptr + t + 1);
+        for (int e = __ldg(tb.sp_ptr + t); e < e1; ++e) {
+            const int ent = __ldg(tb.sp_ent + e);
+            hG += dH[ent >> 2] * dqC[ent];
+        }
+        const double iw = __ldg(tb.inv_mw + t);
+        J[N * (1 + t)] = f * (Q * iw - p.S * Q * __ldg(tb.cp + t) * iw / p.cpm + p.c0 * iw * (hG - hg));
+    }
+    if (t == 0) J[0] = f * p.S * (Q / p.T + dQT);
+    TM::sync();
+    // below the temperature floor f does not depend on T: zero column 0
+    if (!(ys[0] > T_FLOOR) && t < N) J[t] = 0.0;
+    TM::sync();
+}
+
+// Mechanism object used by the integrators: block teams, one element per thread.
 template <int KS>
 struct MassAction {
     static constexpr int K = KS;
@@ -68,222 +277,16 @@ struct MassAction {
     static int smem_rhs(int R) { return N + 3 * K + R; }
     // jacob scratch doubles (may alias the complex Radau matrix): ys, C, h, grt, q, dqdT, dH, dqdC[4]
     static int smem_jac(int R) { return N + 3 * K + 7 * R; }
-    MassActionTables tb;
-
-    struct Prep {
-        double T, S, c0, cpm, logT, log_catm;
-    };
 
     template <int TS>
-    __device__ __forceinline__ Prep prepare(double P, const Vec<N, TS>& y, double* ys, double* C, double* h,
-                                            double* grt) const {
-        using TM = Team<TS>;
-        const int lane = TM::lane();
-#pragma unroll
-        for (int s = 0; s < Vec<N, TS>::S; ++s)
-            if (Vec<N, TS>::ok(s)) ys[Vec<N, TS>::idx(s)] = y[s];
-        TM::sync();
-        Prep p;
-        p.T = fmax(ys[0], T_FLOOR);
-        double S = 0.0, cpm = 0.0;
-        for (int k = lane; k < K; k += TS) {
-            const double yk = ys[1 + k] * __ldg(tb.inv_mw + k);
-            S += yk;
-            cpm += yk * __ldg(tb.cp + k);
-        }
-        p.S = TM::sum(S);
-        p.cpm = TM::sum(cpm);
-        p.c0 = 1e-6 * P / (R_U * p.T);
-        p.logT = log(p.T);
-        p.log_catm = log(1e-6 * P_ATM / (R_U * p.T));
-        const double lnt = log(p.T / T_REF);
-        const double inv_rt = 1.0 / (R_U * p.T);
-        const double c0s = p.c0 / p.S;
-        for (int k = lane; k < K; k += TS) {
-            C[k] = c0s * (ys[1 + k] * __ldg(tb.inv_mw + k));
-            const double cpk = __ldg(tb.cp + k);
-            const double hk = __ldg(tb.h_form + k) + cpk * (p.T - T_REF);
-            h[k] = hk;
-            grt[k] = hk * inv_rt - (__ldg(tb.s_ref + k) + cpk * lnt) * (1.0 / R_U);
-        }
-        TM::sync();
-        return p;
+    __device__ __forceinline__ void dydt(double, double P, const Vec<N, TS>& y, Vec<N, TS>& dy, double* sm) const {
+        static_assert(Team<TS>::block && Vec<N, TS>::S == 1, "mass action runs on block teams, one element per thread");
+        dy[0] = ma_dydt<K, TS>(P, y[0], sm);
     }
-
-    // forward / reverse rate constants in log space (one exp each)
-    __device__ __forceinline__ void rates(int r, const Prep& p, const double* grt, int4 sp, double& kf,
-                                          double& kr, int& nre, int& npd) const {
-        double g = grt[sp.z] - grt[sp.x];
-        nre = 1;
-        npd = 1;
-        if (sp.y >= 0) { g -= grt[sp.y]; nre = 2; }
-        if (sp.w >= 0) { g += grt[sp.w]; npd = 2; }
-        const double lkf = __ldg(tb.log_a + r) + __ldg(tb.beta + r) * p.logT - __ldg(tb.ta + r) / p.T;
-        kf = exp(lkf);
-        kr = exp(lkf + g - double(npd - nre) * p.log_catm);
-    }
-
     template <int TS>
-    __device__ void dydt(double, double P, const Vec<N, TS>& y, Vec<N, TS>& dy, double* sm) const {
-        using TM = Team<TS>;
-        const int lane = TM::lane();
-        double* ys = sm;
-        double* C = ys + N;
-        double* h = C + K;
-        double* grt = h + K;
-        double* q = grt + K;
-        const int R = tb.R;
-        const Prep p = prepare<TS>(P, y, ys, C, h, grt);
-        for (int r = lane; r < R; r += TS) {
-            const int4 sp = __ldg(tb.rsp + r);
-            double kf, kr;
-            int nre, npd;
-            rates(r, p, grt, sp, kf, kr, nre, npd);
-            double fwd = kf * C[sp.x];
-            if (nre == 2) fwd *= C[sp.y];
-            double rev = kr * C[sp.z];
-            if (npd == 2) rev *= C[sp.w];
-            q[r] = fwd - rev;
-        }
-        TM::sync();
-        double Qp = 0.0;
-        const double scale = p.S / p.c0;
-#pragma unroll
-        for (int s = 0; s < Vec<N, TS>::S; ++s) {
-            const int i = Vec<N, TS>::idx(s);
-            if (i >= 1 && i < N) {
-                const int k = i - 1;
-                double w = 0.0;
-                const int e1 = __ldg(tb.sp_ptr + k + 1);
-                for (int e = __ldg(tb.sp_ptr + k); e < e1; ++e) {
-                    const int ent = __ldg(tb.sp_ent + e);
-                    const double qr = q[ent >> 2];
-                    w = (ent & 3) < 2 ? w - qr : w + qr;
-                }
-                Qp += h[k] * w;
-                dy[s] = __ldg(tb.mw + k) * scale * w;
-            }
-        }
-        const double Q = TM::sum(Qp);
-        if (lane == 0) dy[0] = -p.S * Q / (p.c0 * p.cpm);
-        TM::sync();
-    }
-
-    // Analytic Jacobian into column-major J (global or shared memory).
-    template <int TS>
-    __device__ void jacob(double, double P, const Vec<N, TS>& y, double* J, double* sm) const {
-        using TM = Team<TS>;
-        const int lane = TM::lane();
-        double* ys = sm;
-        double* C = ys + N;
-        double* h = C + K;
-        double* grt = h + K;
-        double* q = grt + K;
-        double* dqT = q + tb.R;
-        double* dH = dqT + tb.R;
-        const int R = tb.R;
-        double* dqC = dH + R;   // [R][4]
-        const Prep p = prepare<TS>(P, y, ys, C, h, grt);
-        for (int r = lane; r < R; r += TS) {
-            const int4 sp = __ldg(tb.rsp + r);
-            double kf, kr;
-            int nre, npd;
-            rates(r, p, grt, sp, kf, kr, nre, npd);
-            const double c_r0 = C[sp.x], c_r1 = nre == 2 ? C[sp.y] : 1.0;
-            const double c_p0 = C[sp.z], c_p1 = npd == 2 ? C[sp.w] : 1.0;
-            const double fwd = kf * c_r0 * c_r1;
-            const double rev = kr * c_p0 * c_p1;
-            double dh = h[sp.z] - h[sp.x];
-            if (npd == 2) dh += h[sp.w];
-            if (nre == 2) dh -= h[sp.y];
-            const double dlkf = (__ldg(tb.beta + r) + __ldg(tb.ta + r) / p.T) / p.T;
-            const double dlkr = dlkf - dh / (R_U * p.T * p.T) + double(npd - nre) / p.T;
-            q[r] = fwd - rev;
-            dqT[r] = fwd * dlkf - rev * dlkr - (nre * fwd - npd * rev) / p.T;
-            dH[r] = dh;
-            dqC[4 * r + 0] = kf * c_r1;
-            dqC[4 * r + 1] = nre == 2 ? kf * c_r0 : 0.0;
-            dqC[4 * r + 2] = -kr * c_p1;
-            dqC[4 * r + 3] = npd == 2 ? -kr * c_p0 : 0.0;
-        }
-        TM::sync();
-        // species rows (lane owns rows 1 + k); x_m = C_m / c0
-        const double inv_c0 = 1.0 / p.c0;
-        double hgp = 0.0, Qp = 0.0, dQTp = 0.0;
-        constexpr int S = Vec<N, TS>::S;
-        double wk[S], wTk[S], gk[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            wk[s] = wTk[s] = gk[s] = 0.0;
-            const int i = Vec<N, TS>::idx(s);
-            if (i >= 1 && i < N) {
-                const int k = i - 1;
-                double w = 0.0, wT = 0.0, g = 0.0;
-                const int e1 = __ldg(tb.sp_ptr + k + 1);
-                for (int e = __ldg(tb.sp_ptr + k); e < e1; ++e) {
-                    const int ent = __ldg(tb.sp_ent + e);
-                    const int r = ent >> 2;
-                    const double nu = (ent & 3) < 2 ? -1.0 : 1.0;
-                    const int4 sp = __ldg(tb.rsp + r);
-                    w += nu * q[r];
-                    wT += nu * dqT[r];
-                    double gr = dqC[4 * r + 0] * C[sp.x] + dqC[4 * r + 2] * C[sp.z];
-                    if (sp.y >= 0) gr += dqC[4 * r + 1] * C[sp.y];
-                    if (sp.w >= 0) gr += dqC[4 * r + 3] * C[sp.w];
-                    g += nu * gr * inv_c0;
-                }
-                wk[s] = w;
-                wTk[s] = wT;
-                gk[s] = g;
-                hgp += h[k] * g;
-                Qp += h[k] * w;
-                dQTp += __ldg(tb.cp + k) * w + h[k] * wT;
-            }
-        }
-        // dense part of the species rows, then the sparse G entries (each lane touches only its rows)
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const int i = Vec<N, TS>::idx(s);
-            if (i >= 1 && i < N) {
-                const int k = i - 1;
-                const double a = wk[s] * inv_c0 - gk[s];
-                const double wmk = __ldg(tb.mw + k);
-                for (int j = 0; j < K; ++j) J[i + N * (1 + j)] = wmk * __ldg(tb.inv_mw + j) * a;
-                J[i] = (wmk * p.S * inv_c0) * (wTk[s] + wk[s] / p.T);
-                const int e1 = __ldg(tb.sp_ptr + k + 1);
-                for (int e = __ldg(tb.sp_ptr + k); e < e1; ++e) {
-                    const int ent = __ldg(tb.sp_ent + e);
-                    const int r = ent >> 2;
-                    const double nu = (ent & 3) < 2 ? -1.0 : 1.0;
-                    const int4 sp = __ldg(tb.rsp + r);
-                    J[i + N * (1 + sp.x)] += wmk * __ldg(tb.inv_mw + sp.x) * nu * dqC[4 * r + 0];
-                    if (sp.y >= 0) J[i + N * (1 + sp.y)] += wmk * __ldg(tb.inv_mw + sp.y) * nu * dqC[4 * r + 1];
-                    J[i + N * (1 + sp.z)] += wmk * __ldg(tb.inv_mw + sp.z) * nu * dqC[4 * r + 2];
-                    if (sp.w >= 0) J[i + N * (1 + sp.w)] += wmk * __ldg(tb.inv_mw + sp.w) * nu * dqC[4 * r + 3];
-                }
-            }
-        }
-        const double hg = TM::sum(hgp);
-        const double Q = TM::sum(Qp);
-        const double dQT = TM::sum(dQTp);
-        // temperature row: column j gathers sum_r dH_r dq_r/dC_j over the reactions of species j
-        const double f = -1.0 / (p.c0 * p.cpm);
-        for (int j = lane; j < K; j += TS) {
-            double hG = 0.0;
-            const int e1 = __ldg(tb.sp_ptr + j + 1);
-            for (int e = __ldg(tb.sp_ptr + j); e < e1; ++e) {
-                const int ent = __ldg(tb.sp_ent + e);
-                hG += dH[ent >> 2] * dqC[ent];
-            }
-            const double iw = __ldg(tb.inv_mw + j);
-            J[N * (1 + j)] = f * (Q * iw - p.S * Q * __ldg(tb.cp + j) * iw / p.cpm + p.c0 * iw * (hG - hg));
-        }
-        if (lane == 0) J[0] = f * p.S * (Q / p.T + dQT);
-        TM::sync();
-        if (!(ys[0] > T_FLOOR)) {
-            for (int i = lane; i < N; i += TS) J[i] = 0.0;
-        }
-        TM::sync();
+    __device__ __forceinline__ void jacob(double, double P, const Vec<N, TS>& y, double* J, double* sm) const {
+        static_assert(Team<TS>::block && Vec<N, TS>::S == 1, "mass action runs on block teams, one element per thread");
+        ma_jacob<K, TS>(P, y[0], J, sm);
     }
 };
 

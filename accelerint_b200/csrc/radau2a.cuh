@@ -13,6 +13,7 @@
 #pragma once
 #include "common.cuh"
 #include "linalg.cuh"
+#include "wlinalg.cuh"
 
 namespace aib {
 
@@ -72,6 +73,7 @@ constexpr double ELO = 4;
 // Matrix storage of one team: shared memory for teams of several lanes (J may
 // live in global scratch), registers/local memory for a thread per system.
 template <int N, typename LT> struct RadauRegStore {
+    using E1T = LT;
     double J[N * N];
     LT E1[N * N];
     cx<LT> E2[N * N];
@@ -91,20 +93,24 @@ template <int N, typename LT> struct RadauRegStore {
     __device__ double* scratch_jac() { return nullptr; }
 };
 
-template <int N, typename LT> struct RadauTeamStore {
+// L1 is the precision of E1 (the matrix of the error estimate), LT that of E2.
+template <int N, typename LT, typename L1 = LT> struct RadauTeamStore {
+    using E1T = L1;
     double* J;        // N*N (global scratch)
-    LT* E1;           // N*N
+    L1* E1;           // N*N
     cx<LT>* E2;       // N*N (also the Jacobian evaluation scratch)
-    LT* d1;
+    L1* d1;
     cx<LT>* d2;
     int* p1;
     int* p2;
-    double* buf;      // N
+    double* buf;      // 3N (right-hand sides of the block-team solves)
     double* rhs;      // mechanism dydt scratch
+    int* inf;         // 2 (factorisation status of E1, E2)
+    __device__ int* infos() { return inf; }
     __device__ double* jac() { return J; }
-    __device__ LT* e1() { return E1; }
+    __device__ L1* e1() { return E1; }
     __device__ cx<LT>* e2() { return E2; }
-    __device__ LT* dinv1() { return d1; }
+    __device__ L1* dinv1() { return d1; }
     __device__ cx<LT>* dinv2() { return d2; }
     __device__ int* perm1() { return p1; }
     __device__ int* perm2() { return p2; }
@@ -126,6 +132,7 @@ template <int N, int TS, class Mech, typename LT, class Store>
 struct Radau {
     using V = Vec<N, TS>;
     using TM = Team<TS>;
+    using L1 = typename Store::E1T;
     static constexpr int S = V::S;
 
     const Mech& mech;
@@ -151,21 +158,57 @@ struct Radau {
     // radau2a.c:256-278; returns info (0 on success)
     __device__ int decomp(double H) {
         const double* J = st.jac();
-        LT* E1 = st.e1();
+        L1* E1 = st.e1();
         cx<LT>* E2 = st.e2();
         const double g = radau::GAMMA / H, ar = radau::ALPHA / H, ai = radau::BETA / H;
         const int lane = TM::lane();
         for (int e = lane; e < N * N; e += TS) {
             const int i = e % N, j = e / N;
             const double mj = -J[e];
-            E1[e] = LT(i == j ? mj + g : mj);
+            E1[e] = L1(i == j ? mj + g : mj);
             E2[e] = cx<LT>{LT(i == j ? mj + ar : mj), LT(i == j ? ai : 0.0)};
         }
         TM::sync();
         stats.c[ST_DECOMP]++;
-        int info = lu_real<N, TS, LT>(E1, st.perm1(), st.dinv1());
-        if (info != 0) return info;
-        return lu_cplx<N, TS, LT>(E2, st.perm2(), st.dinv2());
+        if constexpr (Team<TS>::block) {
+            // warp 0 factors E1 while warp 1 factors E2 (one warp does both in a 32-thread team)
+            int* inf = st.infos();
+            const int w = TM::warp();
+            const bool l0 = (threadIdx.x & 31) == 0;
+            if (TS >= 64) {
+                if (w == 0) {
+                    const int i1 = wlu_real<N, L1>(E1, st.perm1(), st.dinv1());
+                    if (l0) inf[0] = i1;
+                } else if (w == 1) {
+                    const int i2 = wlu_cplx<N, LT>(E2, st.perm2(), st.dinv2());
+                    if (l0) inf[1] = i2;
+                }
+            } else {
+                const int i1 = wlu_real<N, L1>(E1, st.perm1(), st.dinv1());
+                const int i2 = wlu_cplx<N, LT>(E2, st.perm2(), st.dinv2());
+                if (l0) { inf[0] = i1; inf[1] = i2; }
+            }
+            TM::sync();
+            const int info = inf[0] != 0 ? inf[0] : inf[1];
+            TM::sync();
+            return info;
+        } else {
+            int info = lu_real<N, TS, LT>(E1, st.perm1(), st.dinv1());
+            if (info != 0) return info;
+            return lu_cplx<N, TS, LT>(E2, st.perm2(), st.dinv2());
+        }
+    }
+
+    // Block teams: E1 x = b through the shared buffer, solved by warp 0.
+    __device__ void block_solve_e1(V& x) {
+        double* xb = st.vbuf();
+        const int t = TM::lane();
+        if (t < N) xb[t] = x[0];
+        TM::sync();
+        if (TM::warp() == 0) wsolve_real<N, L1>(st.e1(), st.dinv1(), st.perm1(), xb);
+        TM::sync();
+        if (t < N) x[0] = xb[t];
+        TM::sync();
     }
 
     // radau2a.c:388-441: Z <- T (E^-1 ((1/h) T^-1 A^-1 Z))
@@ -178,10 +221,35 @@ struct Radau {
             R3[s] = radau::TIA(2, 0) * x1 + radau::TIA(2, 1) * x2 + radau::TIA(2, 2) * x3;
         }
         double* buf = st.vbuf();
-        permute<N, TS>(R1, st.perm1(), buf);
-        permute<N, TS>(R2, st.perm2(), buf);
-        permute<N, TS>(R3, st.perm2(), buf);
-        lu_solve_pair<N, TS, LT>(st.e1(), st.dinv1(), R1, st.e2(), st.dinv2(), R2, R3);
+        if constexpr (Team<TS>::block) {
+            const int t = TM::lane();
+            if (t < N) {
+                buf[t] = R1[0];
+                buf[N + t] = R2[0];
+                buf[2 * N + t] = R3[0];
+            }
+            TM::sync();
+            const int w = TM::warp();
+            if (TS >= 64) {
+                if (w == 0) wsolve_real<N, L1>(st.e1(), st.dinv1(), st.perm1(), buf);
+                else if (w == 1) wsolve_cplx<N, LT>(st.e2(), st.dinv2(), st.perm2(), buf + N, buf + 2 * N);
+            } else {
+                wsolve_real<N, L1>(st.e1(), st.dinv1(), st.perm1(), buf);
+                wsolve_cplx<N, LT>(st.e2(), st.dinv2(), st.perm2(), buf + N, buf + 2 * N);
+            }
+            TM::sync();
+            if (t < N) {
+                R1[0] = buf[t];
+                R2[0] = buf[N + t];
+                R3[0] = buf[2 * N + t];
+            }
+            TM::sync();
+        } else {
+            permute<N, TS>(R1, st.perm1(), buf);
+            permute<N, TS>(R2, st.perm2(), buf);
+            permute<N, TS>(R3, st.perm2(), buf);
+            lu_solve_pair<N, TS, LT>(st.e1(), st.dinv1(), R1, st.e2(), st.dinv2(), R2, R3);
+        }
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const double x1 = R1[s], x2 = R2[s], x3 = R3[s];
@@ -194,14 +262,36 @@ struct Radau {
     // E1 x = b with one FP64 refinement step when the factors are single precision.
     __device__ void solve_e1(double H, V& x) {
         double* buf = st.vbuf();
+        if constexpr (Team<TS>::block) {
+            if (sizeof(L1) == sizeof(double)) {
+                block_solve_e1(x);
+                return;
+            }
+            // single-precision factors: one refinement step r = b - ((gamma/h) x - J x) in FP64
+            const V b = x;
+            block_solve_e1(x);
+            const int t = TM::lane();
+            if (t < N) buf[t] = x[0];
+            TM::sync();
+            const double* J = st.jac();
+            double jx = 0.0;
+            if (t < N)
+                for (int j = 0; j < N; ++j) jx = fma(J[t + N * j], buf[j], jx);
+            V r;
+            r[0] = t < N ? b[0] - ((radau::GAMMA / H) * x[0] - jx) : 0.0;
+            TM::sync();
+            block_solve_e1(r);
+            x[0] += r[0];
+            return;
+        }
         if (sizeof(LT) == sizeof(double)) {
             permute<N, TS>(x, st.perm1(), buf);
-            lu_solve_real<N, TS, LT>(st.e1(), st.dinv1(), x);
+            lu_solve_real<N, TS, L1>(st.e1(), st.dinv1(), x);
             return;
         }
         V b = x;
         permute<N, TS>(x, st.perm1(), buf);
-        lu_solve_real<N, TS, LT>(st.e1(), st.dinv1(), x);
+        lu_solve_real<N, TS, L1>(st.e1(), st.dinv1(), x);
         // r = b - ((gamma/h) x - J x)
         const double g = radau::GAMMA / H;
 #pragma unroll
@@ -222,7 +312,7 @@ struct Radau {
         }
         TM::sync();
         permute<N, TS>(r, st.perm1(), buf);
-        lu_solve_real<N, TS, LT>(st.e1(), st.dinv1(), r);
+        lu_solve_real<N, TS, L1>(st.e1(), st.dinv1(), r);
 #pragma unroll
         for (int s = 0; s < S; ++s) x[s] += r[s];
     }

@@ -1,0 +1,321 @@
+// Warp-level dense LU factorisation and solves for block teams: one warp per
+// matrix (32 lanes, rows i = lane + 32 r), the matrix column-major in shared
+// memory.  In a two-warp team warp 0 works on E1 while warp 1 works on E2.
+//
+// Semantics of LAPACK's unblocked xGETF2 / xGETRS as in linalg.cuh (first
+// maximal pivot by |a| or |Re a| + |Im a|, reciprocal scaling of the
+// multiplier column, info = k + 1 on a zero pivot), the radau2a/radau2a.c:
+// 273-277 and :404-417 calls.  The routines are out of line so the team kernel
+// holds one copy of each: a fully inlined integrator does not fit the
+// instruction cache.
+#pragma once
+#include "common.cuh"
+
+namespace aib {
+
+template <int R, typename V> __device__ __forceinline__ double vsel(const V& x, int s) {
+    double r = x[0];
+#pragma unroll
+    for (int k = 1; k < R; ++k)
+        if (s == k) r = x[k];
+    return r;
+}
+template <int R, typename V> __device__ __forceinline__ void vput(V& x, int s, double v) {
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+        if (s == k) x[k] = v;
+}
+
+__device__ __forceinline__ double dbl(double a) { return a; }
+__device__ __forceinline__ double dbl(float a) { return double(a); }
+
+// Real LU in place; perm[i] = original row at position i, dinv[k] = 1 / U(k,k).
+template <int N, typename T>
+__device__ __noinline__ int wlu_real(T* A, int* perm, T* dinv)
+{
+    constexpr int R = (N + 31) / 32;
+    constexpr int CB = 8;
+    const int lane = threadIdx.x & 31;
+    int info = 0;
+    for (int i = lane; i < N; i += 32) perm[i] = i;
+    __syncwarp();
+#pragma unroll 1
+    for (int k = 0; k < N; ++k) {
+        double best = -1.0;
+        int bi = 0x7fffffff;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            if (i >= k && i < N) {
+                const double a = fabs(dbl(A[i + k * N]));
+                if (!(a <= best)) { best = a; bi = i; }   // NaN-safe: a row is always taken
+            }
+        }
+        const int p = Team<32>::argmax(best, bi);
+        const T piv = A[p + k * N];
+        if (piv != T(0)) {
+            if (p != k) {
+                for (int j = lane; j < N; j += 32) {
+                    const T t = A[k + j * N];
+                    A[k + j * N] = A[p + j * N];
+                    A[p + j * N] = t;
+                }
+                if (lane == 0) { const int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
+                __syncwarp();
+            }
+            const T rc = T(1) / piv;
+            if (lane == 0) dinv[k] = rc;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = lane + 32 * r;
+                if (i > k && i < N) A[i + k * N] *= rc;
+            }
+        } else {
+            if (info == 0) info = k + 1;
+            if (lane == 0) dinv[k] = T(0);
+        }
+        __syncwarp();
+        T l[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            l[r] = (i > k && i < N) ? A[i + k * N] : T(0);
+        }
+        // trailing update in column chunks: the loads of a chunk are in flight together
+#pragma unroll 1
+        for (int j0 = k + 1; j0 < N; j0 += CB) {
+            T u[CB], a[R][CB];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) u[c] = (j0 + c < N) ? A[k + (j0 + c) * N] : T(0);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = lane + 32 * r;
+#pragma unroll
+                for (int c = 0; c < CB; ++c)
+                    a[r][c] = (i > k && i < N && j0 + c < N) ? A[i + (j0 + c) * N] : T(0);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = lane + 32 * r;
+#pragma unroll
+                for (int c = 0; c < CB; ++c)
+                    if (i > k && i < N && j0 + c < N) A[i + (j0 + c) * N] = fma(l[r], -u[c], a[r][c]);
+            }
+        }
+        __syncwarp();
+    }
+    return info;
+}
+
+template <int N, typename T>
+__device__ __noinline__ int wlu_cplx(cx<T>* A, int* perm, cx<T>* dinv)
+{
+    constexpr int R = (N + 31) / 32;
+    constexpr int CB = 4;
+    const int lane = threadIdx.x & 31;
+    const cx<T> z{T(0), T(0)};
+    int info = 0;
+    for (int i = lane; i < N; i += 32) perm[i] = i;
+    __syncwarp();
+#pragma unroll 1
+    for (int k = 0; k < N; ++k) {
+        double best = -1.0;
+        int bi = 0x7fffffff;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            if (i >= k && i < N) {
+                const double a = dbl(cabs1(A[i + k * N]));
+                if (!(a <= best)) { best = a; bi = i; }
+            }
+        }
+        const int p = Team<32>::argmax(best, bi);
+        const cx<T> piv = A[p + k * N];
+        if (piv.re != T(0) || piv.im != T(0)) {
+            if (p != k) {
+                for (int j = lane; j < N; j += 32) {
+                    const cx<T> t = A[k + j * N];
+                    A[k + j * N] = A[p + j * N];
+                    A[p + j * N] = t;
+                }
+                if (lane == 0) { const int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
+                __syncwarp();
+            }
+            const cx<T> rc = crecip(piv);
+            if (lane == 0) dinv[k] = rc;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = lane + 32 * r;
+                if (i > k && i < N) A[i + k * N] = cmul(A[i + k * N], rc);
+            }
+        } else {
+            if (info == 0) info = k + 1;
+            if (lane == 0) dinv[k] = z;
+        }
+        __syncwarp();
+        cx<T> l[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            l[r] = (i > k && i < N) ? A[i + k * N] : z;
+        }
+#pragma unroll 1
+        for (int j0 = k + 1; j0 < N; j0 += CB) {
+            cx<T> u[CB], a[R][CB];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) u[c] = (j0 + c < N) ? A[k + (j0 + c) * N] : z;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = lane + 32 * r;
+#pragma unroll
+                for (int c = 0; c < CB; ++c) a[r][c] = (i > k && i < N && j0 + c < N) ? A[i + (j0 + c) * N] : z;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = lane + 32 * r;
+#pragma unroll
+                for (int c = 0; c < CB; ++c)
+                    if (i > k && i < N && j0 + c < N) A[i + (j0 + c) * N] = cfnma(l[r], u[c], a[r][c]);
+            }
+        }
+        __syncwarp();
+    }
+    return info;
+}
+
+// Solve (P^T L U) x = b in place on a shared-memory vector xb[N] (b in, x out):
+// gather by perm, unit-lower forward and upper backward substitution with the
+// reciprocal diagonal, x held in registers, the next factor column loaded
+// while the current one is applied.  (A zero entry of x is not skipped as
+// dtrsm does; the update by an exact zero leaves finite values unchanged.)
+template <int N, typename T>
+__device__ __noinline__ void wsolve_real(const T* A, const T* dinv, const int* perm, double* xb)
+{
+    constexpr int R = (N + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    double x[R];
+    T cur[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        x[r] = i < N ? xb[perm[i]] : 0.0;
+        cur[r] = (i > 0 && i < N) ? A[i] : T(0);
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int j = 0; j < N; ++j) {
+        T nxt[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            nxt[r] = (j + 1 < N && i > j + 1 && i < N) ? A[i + (j + 1) * N] : T(0);
+        }
+        const double xj = __shfl_sync(0xffffffffu, vsel<R>(x, j >> 5), j & 31);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            x[r] = fma(-xj, dbl(cur[r]), x[r]);
+            cur[r] = nxt[r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        cur[r] = (i < N - 1) ? A[i + (N - 1) * N] : T(0);
+    }
+#pragma unroll 1
+    for (int j = N - 1; j >= 0; --j) {
+        T nxt[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            nxt[r] = (j > 0 && i < j - 1) ? A[i + (j - 1) * N] : T(0);
+        }
+        const double xv = vsel<R>(x, j >> 5) * dbl(dinv[j]);
+        if (lane == (j & 31)) vput<R>(x, j >> 5, xv);
+        const double xj = __shfl_sync(0xffffffffu, xv, j & 31);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            x[r] = fma(-xj, dbl(cur[r]), x[r]);
+            cur[r] = nxt[r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        if (i < N) xb[i] = x[r];
+    }
+    __syncwarp();
+}
+
+template <int N, typename T>
+__device__ __noinline__ void wsolve_cplx(const cx<T>* A, const cx<T>* dinv, const int* perm, double* xbr,
+                                         double* xbi)
+{
+    constexpr int R = (N + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const cx<T> z{T(0), T(0)};
+    double xr[R], xi[R];
+    cx<T> cur[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        xr[r] = i < N ? xbr[perm[i]] : 0.0;
+        xi[r] = i < N ? xbi[perm[i]] : 0.0;
+        cur[r] = (i > 0 && i < N) ? A[i] : z;
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int j = 0; j < N; ++j) {
+        cx<T> nxt[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            nxt[r] = (j + 1 < N && i > j + 1 && i < N) ? A[i + (j + 1) * N] : z;
+        }
+        const double br = __shfl_sync(0xffffffffu, vsel<R>(xr, j >> 5), j & 31);
+        const double bi = __shfl_sync(0xffffffffu, vsel<R>(xi, j >> 5), j & 31);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double lr = dbl(cur[r].re), li = dbl(cur[r].im);
+            xr[r] = fma(bi, li, fma(-br, lr, xr[r]));
+            xi[r] = fma(-bi, lr, fma(-br, li, xi[r]));
+            cur[r] = nxt[r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        cur[r] = (i < N - 1) ? A[i + (N - 1) * N] : z;
+    }
+#pragma unroll 1
+    for (int j = N - 1; j >= 0; --j) {
+        cx<T> nxt[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            nxt[r] = (j > 0 && i < j - 1) ? A[i + (j - 1) * N] : z;
+        }
+        const cx<T> dv = dinv[j];
+        const double ar = vsel<R>(xr, j >> 5), ai = vsel<R>(xi, j >> 5);
+        const double nr = ar * dbl(dv.re) - ai * dbl(dv.im);
+        const double ni = ar * dbl(dv.im) + ai * dbl(dv.re);
+        if (lane == (j & 31)) { vput<R>(xr, j >> 5, nr); vput<R>(xi, j >> 5, ni); }
+        const double br = __shfl_sync(0xffffffffu, nr, j & 31);
+        const double bi = __shfl_sync(0xffffffffu, ni, j & 31);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double ur = dbl(cur[r].re), ui = dbl(cur[r].im);
+            xr[r] = fma(bi, ui, fma(-br, ur, xr[r]));
+            xi[r] = fma(-bi, ur, fma(-br, ui, xi[r]));
+            cur[r] = nxt[r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        if (i < N) { xbr[i] = xr[r]; xbi[i] = xi[r]; }
+    }
+    __syncwarp();
+}
+
+}  // namespace aib

@@ -69,7 +69,9 @@ void accelerInt_cleanup(void);
 
 /* precision of the Radau simplified-Newton matrices E1/E2 */
 #define ACCELERINT_LU_FP64 0
-#define ACCELERINT_LU_FP32 1   /* factor + solve in FP32; residuals, error estimate, control in FP64 */
+#define ACCELERINT_LU_FP32 1       /* complex E2 factored + solved in FP32, real E1 (error estimate) in FP64;
+                                      residuals, error estimate, step control in FP64 */
+#define ACCELERINT_LU_FP32_ALL 2   /* E1 and E2 in FP32; the error-estimate solve gets one FP64 refinement step */
 
 /* Synthetic constant-pressure mass-action mechanism (plain tables; see
  * accelerint_b200/mechanism.py for the model).  Stands in for the pyJac

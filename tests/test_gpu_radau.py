@@ -3,7 +3,7 @@ radau2a/radau2a.c), through the C-ABI (accelerInt_integrate_status)."""
 import numpy as np
 import pytest
 
-from accelerint_b200 import (LU_FP32, LU_FP64, Integrator, VanDerPol, mechanism_13, mechanism_53,
+from accelerint_b200 import (LU_FP32, LU_FP32_ALL, LU_FP64, Integrator, VanDerPol, mechanism_13, mechanism_53,
                              mass_action_initial_conditions, mixed_stiffness_initial_conditions,
                              vdp_initial_conditions)
 from tests.helpers import check_parity, per_system_error, perturbed, weighted_error
@@ -38,32 +38,37 @@ def test_van_der_pol(oracle, lu):
         assert eg.max() <= 3.0 * eo.max() + 1.0
 
 
-@pytest.mark.parametrize("lu", [LU_FP64, LU_FP32])
+def check_mass_action(yg, yo, yp, yt, lu):
+    """FP64: agreement with the reference CPU solver within its own perturbation envelope.
+    Single-precision factorisations change Newton convergence, hence the step sequence;
+    they must then be as accurate as the FP64 reference against the tight oracle."""
+    if lu == LU_FP64:
+        check_parity(yg, yo, yp)
+    eg, eo = per_system_error(yg, yt), per_system_error(yo, yt)
+    assert not np.isnan(yg).any()
+    assert np.median(eg) <= 1.5 * np.median(eo) + 1.0
+    assert eg.max() <= 2.0 * eo.max() + 1.0
+
+
+@pytest.mark.parametrize("lu", [LU_FP64, LU_FP32, LU_FP32_ALL])
 def test_mass_action_14(oracle, lu):
     mech = mechanism_13()
     y, var = mass_action_initial_conditions(mech, 256, seed=11)
     yg, cg = run_gpu(mech, y, var, 0.0, 5e-6, 1e-6, lu=lu)
     yo, co, _ = oracle.run("radau2a", mech, y, var, 0.0, 5e-6, 1e-6)
     yp, _, _ = oracle.run("radau2a", mech, perturbed(y), var, 0.0, 5e-6, 1e-6)
-    assert (co == 0).all() and (cg == 0).all()
-    check_parity(yg, yo, yp)
-    # as accurate as the reference CPU solver against a tight FP64 oracle (rtol 1e-12)
     yt, _, _ = oracle.run("radau2a", mech, y, var, 0.0, 5e-6, 1e-6, rtol=1e-12, atol=1e-20)
-    eg, eo = per_system_error(yg, yt), per_system_error(yo, yt)
-    assert np.median(eg) <= 2.0 * np.median(eo) + 1.0
-    assert eg.max() <= 3.0 * eo.max() + 1.0
+    assert (co == 0).all() and (cg == 0).all()
+    check_mass_action(yg, yo, yp, yt, lu)
 
 
-@pytest.mark.parametrize("lu", [LU_FP64, LU_FP32])
+@pytest.mark.parametrize("lu", [LU_FP64, LU_FP32, LU_FP32_ALL])
 def test_mass_action_54(oracle, lu):
     mech = mechanism_53()
     y, var = mixed_stiffness_initial_conditions(mech, 64, seed=5)
     yg, cg = run_gpu(mech, y, var, 0.0, 2e-6, 1e-6, lu=lu)
     yo, co, _ = oracle.run("radau2a", mech, y, var, 0.0, 2e-6, 1e-6)
     yp, _, _ = oracle.run("radau2a", mech, perturbed(y), var, 0.0, 2e-6, 1e-6)
-    assert (co == 0).all() and (cg == 0).all()
-    check_parity(yg, yo, yp)
     yt, _, _ = oracle.run("radau2a", mech, y, var, 0.0, 2e-6, 1e-6, rtol=1e-12, atol=1e-20)
-    eg, eo = per_system_error(yg, yt), per_system_error(yo, yt)
-    assert np.median(eg) <= 2.0 * np.median(eo) + 1.0
-    assert eg.max() <= 3.0 * eo.max() + 1.0
+    assert (co == 0).all() and (cg == 0).all()
+    check_mass_action(yg, yo, yp, yt, lu)
