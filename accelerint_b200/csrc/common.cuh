@@ -83,10 +83,14 @@ template <int TS> struct Team {
     __device__ __forceinline__ static int lane() { return TS == 1 ? 0 : int(threadIdx.x & (TS - 1)); }
     __device__ __forceinline__ static int warp() { return block ? int(threadIdx.x >> 5) : 0; }
     __device__ __forceinline__ static unsigned mask() {
-        if (TS >= 32) return 0xffffffffu;
-        if (TS == 1) return 1u << (threadIdx.x & 31);
-        const unsigned base = (threadIdx.x & 31) & ~unsigned(TS - 1);
-        return ((1u << TS) - 1u) << base;
+        if constexpr (TS >= 32) {
+            return 0xffffffffu;
+        } else if constexpr (TS == 1) {
+            return 1u << (threadIdx.x & 31);
+        } else {
+            const unsigned base = (threadIdx.x & 31) & ~unsigned(TS - 1);
+            return ((1u << TS) - 1u) << base;
+        }
     }
     __device__ __forceinline__ static void sync() {
         if (TS > 32) __syncthreads();
