@@ -28,7 +28,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_set_mechanism_mass_action", "accelerInt_set_tolerances",
     "accelerInt_set_lu_precision", "accelerInt_integrate_status", "accelerInt_integrate_device",
     "accelerInt_last_status", "accelerInt_get_codes", "accelerInt_get_poles", "accelerInt_version",
-    "accelerInt_measure_fma_peak",
+    "accelerInt_measure_fma_peak", "accelerInt_integrate_device_noalloc",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -66,6 +66,9 @@ def load_library():
     lib.accelerInt_integrate_device.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.accelerInt_integrate_device_noalloc.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                                        ctypes.c_void_p, ctypes.c_void_p]
     lib.accelerInt_last_status.argtypes = []
     lib.accelerInt_get_codes.argtypes = [_ip, ctypes.c_int]
     lib.accelerInt_get_poles.argtypes = [_dp, _dp, _dp, _dp]

@@ -452,3 +452,115 @@ int accelerInt_measure_fma_peak(int fp64, double* tflops) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.  Its device scratch (the work-queue counter and
+// the per-team Jacobians of the mass-action Radau kernel) lives in this
+// file-scope array instead of memory from cudaMalloc.  Every device that loads
+// the library holds the array until the process exits.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;   // 16 MiB
+constexpr size_t kNoAllocQueueBytes = 256;                   // queue counter + padding
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the array for the current device, looked up once per device.
+// In host code the array's name is only a host-side stand-in, never a device address.
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return ACCELERINT_ERR_ARGUMENT;
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            fprintf(stderr, "accelerint_b200: cudaGetSymbolAddress of the static scratch failed: %s\n",
+                    cudaGetErrorString(e));
+            return ACCELERINT_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return ACCELERINT_OK;
+}
+
+template <int SK, class Mech, int TS, typename LT, typename L1 = LT>
+int launch_team_noalloc(BatchArgs a, const Mech& mech, TeamLayout lay, unsigned char* scratch, cudaStream_t s) {
+    constexpr int N = Mech::N;
+    const size_t per_team = size_t(N) * N * sizeof(double);
+    const size_t fit = (kNoAllocScratchBytes - kNoAllocQueueBytes) / per_team;
+    if (fit < 1) {
+        fprintf(stderr, "accelerint_b200: state length %d needs %zu bytes of scratch per system in flight; "
+                        "the allocation-free entry point holds %zu\n", N, per_team + kNoAllocQueueBytes,
+                kNoAllocScratchBytes);
+        return ACCELERINT_ERR_ARGUMENT;
+    }
+    const int block = TS >= 32 ? TS : 32, tpb = block / TS;
+    const size_t smem = size_t(lay.total) * tpb;
+    auto kern = team_kernel<SK, Mech, TS, LT, L1>;
+    int grid = 0;
+    int rc = persistent_grid(kern, block, smem, a.num, tpb, &grid);
+    if (rc) return rc;
+    // fewer teams in flight when the scratch cannot hold a Jacobian for each (the work queue keeps it correct)
+    grid = int(std::min<size_t>(size_t(grid), fit / size_t(tpb)));
+    if (grid < 1) return ACCELERINT_ERR_ARGUMENT;
+    a.queue = reinterpret_cast<int*>(scratch);
+    a.jac = reinterpret_cast<double*>(scratch + kNoAllocQueueBytes);
+    CK(cudaMemsetAsync(a.queue, 0, sizeof(int), s));   // the counter must start at zero on every call
+    kern<<<grid, block, smem, s>>>(a, mech, lay);
+    CK(cudaGetLastError());
+    return ACCELERINT_OK;
+}
+
+template <int K, int TS>
+int launch_mass_action_noalloc(BatchArgs a, unsigned char* scratch, cudaStream_t s) {
+    using M = MassAction<K>;
+    M mech;
+    const int R = g.mt.R;
+    constexpr int N = M::N;
+    if (g.solver != ACCELERINT_RADAU2A) return ACCELERINT_ERR_UNSUPPORTED;
+    if (g.lu == ACCELERINT_LU_FP32) {
+        TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 8);
+        return launch_team_noalloc<SK_RADAU, M, TS, float, double>(a, mech, lay, scratch, s);
+    }
+    if (g.lu == ACCELERINT_LU_FP32_ALL) {
+        TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 4);
+        return launch_team_noalloc<SK_RADAU, M, TS, float, float>(a, mech, lay, scratch, s);
+    }
+    TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
+    return launch_team_noalloc<SK_RADAU, M, TS, double>(a, mech, lay, scratch, s);
+}
+
+}  // namespace
+
+extern "C" int accelerInt_integrate_device_noalloc(int NUM, double t_start, double t_end, double stepsize,
+                                                   double* y_dev, const double* var_dev, int* codes_dev,
+                                                   void* stream) {
+    if (!g.initialized || g.mech_kind != 1) return ACCELERINT_ERR_STATE;
+    if (NUM < 0 || (NUM > 0 && (!y_dev || !var_dev))) return ACCELERINT_ERR_ARGUMENT;
+    if (NUM == 0) return ACCELERINT_OK;
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    BatchArgs a{};
+    a.num = NUM;
+    a.t_start = t_start;
+    a.t_end = t_end;
+    a.step = stepsize < 0 ? t_end - t_start : stepsize;
+    a.y = y_dev;
+    a.var = var_dev;
+    a.codes = codes_dev;
+    a.stats = nullptr;
+    a.atol = g.atol;
+    a.rtol = g.rtol;
+    unsigned char* sp = static_cast<unsigned char*>(scratch);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch (g.mt.K) {
+        case 13: return launch_mass_action_noalloc<13, 32>(a, sp, st);
+        case 53: return launch_mass_action_noalloc<53, 64>(a, sp, st);
+        default: return ACCELERINT_ERR_UNSUPPORTED;
+    }
+}

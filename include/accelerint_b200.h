@@ -111,6 +111,27 @@ int accelerInt_integrate_device(int NUM, double t_start, double t_end, double st
                                 double* y_dev, const double* var_dev, int* codes_dev,
                                 int* stats_dev, void* stream);
 
+/* Allocation-free form of accelerInt_integrate_device, for hosts that cannot
+ * let a library allocate device memory during a run -- for example a CFD code
+ * that plans all device memory up front or hands out memory from its own pool,
+ * or a caller that must not risk the device-wide synchronisation that
+ * cudaMalloc/cudaFree can imply.  No counterpart in the reference (its
+ * library allocates in accelerInt_initialize).  The caller passes the device
+ * state y_dev[i * NUM + ivp], var_dev[NUM] and optionally codes_dev[NUM];
+ * the integrator's own scratch (a work-queue counter and one N x N Jacobian
+ * per system in flight) lives in a 16 MiB array compiled into the library,
+ * which every GPU that loads the library holds until the process exits.
+ * Limits: mass-action mechanism and Radau only; the number of systems in flight
+ * is capped by what fits in 16 MiB (719 at N = 54, so it can be slower than
+ * accelerInt_integrate_device); a state length whose single N x N Jacobian does
+ * not fit is rejected with ACCELERINT_ERR_ARGUMENT.  The first call on a device
+ * looks up the array's device address; make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.
+ * accelerInt_initialize and the mechanism setters must have run before. */
+int accelerInt_integrate_device_noalloc(int NUM, double t_start, double t_end, double stepsize,
+                                        double* y_dev, const double* var_dev, int* codes_dev, void* stream);
+
 int accelerInt_last_status(void);
 /* Copies the EC_* codes of the last accelerInt_integrate* call (host pointer, NUM entries). */
 int accelerInt_get_codes(int* codes_host, int NUM);
