@@ -103,9 +103,10 @@ struct TeamLayout {
         TeamLayout L;
         int o = 0;
         if (l1_bytes == 0) l1_bytes = lt_bytes;
-        L.e1 = o; o += al(N * N * l1_bytes);
+        const int NC = lu_cols(N);   // padded column count of the block-team factorisation
+        L.e1 = o; o += al(N * NC * l1_bytes);
         L.e2 = o;
-        const int e2b = N * N * 2 * lt_bytes, jb = jac_doubles * 8;
+        const int e2b = N * NC * 2 * lt_bytes, jb = jac_doubles * 8;
         o += al(e2b > jb ? e2b : jb);
         L.d1 = o; o += al(N * l1_bytes);
         L.d2 = o; o += al(N * 2 * lt_bytes);
@@ -127,7 +128,8 @@ struct TeamLayout {
 };
 
 template <int SK, class Mech, int TS, typename LT, typename L1 = LT>
-__global__ void __launch_bounds__(TS >= 32 ? TS : 32) team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
+__global__ void __launch_bounds__(TS >= 32 ? TS : 32, (TS >= 64 && sizeof(L1) == 4) ? 5 : 1)
+team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
 {
     constexpr int N = Mech::N;
     using TM = Team<TS>;

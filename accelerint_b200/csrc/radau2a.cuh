@@ -162,9 +162,11 @@ struct Radau {
         cx<LT>* E2 = st.e2();
         const double g = radau::GAMMA / H, ar = radau::ALPHA / H, ai = radau::BETA / H;
         const int lane = TM::lane();
-        for (int e = lane; e < N * N; e += TS) {
+        // block teams store lu_cols(N) columns, the ones past N zero (see wlinalg.cuh)
+        constexpr int NC = Team<TS>::block ? lu_cols(N) : N;
+        for (int e = lane; e < N * NC; e += TS) {
             const int i = e % N, j = e / N;
-            const double mj = -J[e];
+            const double mj = j < N ? -J[e] : 0.0;
             E1[e] = L1(i == j ? mj + g : mj);
             E2[e] = cx<LT>{LT(i == j ? mj + ar : mj), LT(i == j ? ai : 0.0)};
         }

@@ -26,21 +26,44 @@ template <int R, typename V> __device__ __forceinline__ void vput(V& x, int s, d
         if (s == k) x[k] = v;
 }
 
+// Columns of the stored E1/E2: N rounded up to a multiple of 8; the extra
+// columns (leading dimension N) hold zeros so that factorisation chunks need no
+// bounds tests.
+__host__ __device__ constexpr int lu_cols(int n) { return (n + 7) & ~7; }
+
 __device__ __forceinline__ double dbl(double a) { return a; }
 __device__ __forceinline__ double dbl(float a) { return double(a); }
 
-// Real LU in place; perm[i] = original row at position i, dinv[k] = 1 / U(k,k).
+// First-maximum argmax over the warp for magnitudes m >= 0 (m < 0: no
+// candidate; NaN counts as a candidate).  Two 32-bit warp reductions on the
+// ordered bit pattern, then the smallest row index among the winners.
+__device__ __forceinline__ int warp_pivot(double m, int idx) {
+    unsigned long long b = 0;
+    if (!(m < 0.0)) b = static_cast<unsigned long long>(__double_as_longlong(fabs(m))) + 1ull;
+    const unsigned hi = unsigned(b >> 32), lo = unsigned(b);
+    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    const bool win = b != 0 && hi == mh && lo == ml;
+    const int cand = win ? idx : 0x7fffffff;
+    return int(__reduce_min_sync(0xffffffffu, unsigned(cand)));
+}
+
+// Real LU in place of an N x lu_cols(N) column-major array (zero columns past
+// N); perm[i] = original row at position i, dinv[k] = 1 / U(k,k).
 template <int N, typename T>
 __device__ __noinline__ int wlu_real(T* A, int* perm, T* dinv)
 {
     constexpr int R = (N + 31) / 32;
     constexpr int CB = 8;
+    constexpr int NC = lu_cols(N);
+    static_assert(NC % CB == 0, "column padding");
     const int lane = threadIdx.x & 31;
     int info = 0;
     for (int i = lane; i < N; i += 32) perm[i] = i;
     __syncwarp();
 #pragma unroll 1
     for (int k = 0; k < N; ++k) {
+        // pivot: first maximal |a| in column k, rows k..N-1
         double best = -1.0;
         int bi = 0x7fffffff;
 #pragma unroll
@@ -51,7 +74,7 @@ __device__ __noinline__ int wlu_real(T* A, int* perm, T* dinv)
                 if (!(a <= best)) { best = a; bi = i; }   // NaN-safe: a row is always taken
             }
         }
-        const int p = Team<32>::argmax(best, bi);
+        const int p = warp_pivot(best, bi);
         const T piv = A[p + k * N];
         if (piv != T(0)) {
             if (p != k) {
@@ -76,31 +99,33 @@ __device__ __noinline__ int wlu_real(T* A, int* perm, T* dinv)
         }
         __syncwarp();
         T l[R];
+        bool act[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int i = lane + 32 * r;
-            l[r] = (i > k && i < N) ? A[i + k * N] : T(0);
+            act[r] = i > k && i < N;
+            l[r] = act[r] ? A[i + k * N] : T(0);
         }
-        // trailing update in column chunks: the loads of a chunk are in flight together
+        // Trailing update in chunks of CB columns from a chunk boundary; the storage
+        // is padded with zero columns to a multiple of CB (NC), columns j <= k carry
+        // u = 0, so a chunk needs no bounds tests; only rows below k are written.
+        T* colp = A + lane;
 #pragma unroll 1
-        for (int j0 = k + 1; j0 < N; j0 += CB) {
+        for (int j0 = (k + 1) & ~(CB - 1); j0 < NC; j0 += CB) {
             T u[CB], a[R][CB];
+            const T* pr = A + k + j0 * N;
+            T* pc = colp + j0 * N;
 #pragma unroll
-            for (int c = 0; c < CB; ++c) u[c] = (j0 + c < N) ? A[k + (j0 + c) * N] : T(0);
+            for (int c = 0; c < CB; ++c) u[c] = (j0 + c > k) ? pr[c * N] : T(0);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = lane + 32 * r;
+            for (int r = 0; r < R; ++r)
 #pragma unroll
-                for (int c = 0; c < CB; ++c)
-                    a[r][c] = (i > k && i < N && j0 + c < N) ? A[i + (j0 + c) * N] : T(0);
-            }
+                for (int c = 0; c < CB; ++c) a[r][c] = act[r] ? pc[32 * r + c * N] : T(0);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = lane + 32 * r;
+            for (int r = 0; r < R; ++r)
 #pragma unroll
                 for (int c = 0; c < CB; ++c)
-                    if (i > k && i < N && j0 + c < N) A[i + (j0 + c) * N] = fma(l[r], -u[c], a[r][c]);
-            }
+                    if (act[r]) pc[32 * r + c * N] = fma(l[r], -u[c], a[r][c]);
         }
         __syncwarp();
     }
@@ -111,7 +136,9 @@ template <int N, typename T>
 __device__ __noinline__ int wlu_cplx(cx<T>* A, int* perm, cx<T>* dinv)
 {
     constexpr int R = (N + 31) / 32;
-    constexpr int CB = 4;
+    constexpr int CB = 8;
+    constexpr int NC = lu_cols(N);
+    static_assert(NC % CB == 0, "column padding");
     const int lane = threadIdx.x & 31;
     const cx<T> z{T(0), T(0)};
     int info = 0;
@@ -129,7 +156,7 @@ __device__ __noinline__ int wlu_cplx(cx<T>* A, int* perm, cx<T>* dinv)
                 if (!(a <= best)) { best = a; bi = i; }
             }
         }
-        const int p = Team<32>::argmax(best, bi);
+        const int p = warp_pivot(best, bi);
         const cx<T> piv = A[p + k * N];
         if (piv.re != T(0) || piv.im != T(0)) {
             if (p != k) {
@@ -154,29 +181,30 @@ __device__ __noinline__ int wlu_cplx(cx<T>* A, int* perm, cx<T>* dinv)
         }
         __syncwarp();
         cx<T> l[R];
+        bool act[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int i = lane + 32 * r;
-            l[r] = (i > k && i < N) ? A[i + k * N] : z;
+            act[r] = i > k && i < N;
+            l[r] = act[r] ? A[i + k * N] : z;
         }
+        cx<T>* colp = A + lane;
 #pragma unroll 1
-        for (int j0 = k + 1; j0 < N; j0 += CB) {
+        for (int j0 = (k + 1) & ~(CB - 1); j0 < NC; j0 += CB) {
             cx<T> u[CB], a[R][CB];
+            const cx<T>* pr = A + k + j0 * N;
+            cx<T>* pc = colp + j0 * N;
 #pragma unroll
-            for (int c = 0; c < CB; ++c) u[c] = (j0 + c < N) ? A[k + (j0 + c) * N] : z;
+            for (int c = 0; c < CB; ++c) u[c] = (j0 + c > k) ? pr[c * N] : z;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = lane + 32 * r;
+            for (int r = 0; r < R; ++r)
 #pragma unroll
-                for (int c = 0; c < CB; ++c) a[r][c] = (i > k && i < N && j0 + c < N) ? A[i + (j0 + c) * N] : z;
-            }
+                for (int c = 0; c < CB; ++c) a[r][c] = act[r] ? pc[32 * r + c * N] : z;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = lane + 32 * r;
+            for (int r = 0; r < R; ++r)
 #pragma unroll
                 for (int c = 0; c < CB; ++c)
-                    if (i > k && i < N && j0 + c < N) A[i + (j0 + c) * N] = cfnma(l[r], u[c], a[r][c]);
-            }
+                    if (act[r]) pc[32 * r + c * N] = cfnma(l[r], u[c], a[r][c]);
         }
         __syncwarp();
     }

@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--lu", default="fp32", choices=["fp32", "fp64"])
+    p.add_argument("--lu", default="fp32", choices=["fp32", "fp32_all", "fp64"])
     p.add_argument("--num", type=int, default=1 << 20)
     p.add_argument("--solver", default="radau2a")
     p.add_argument("--seed", type=int, default=2024)
@@ -206,7 +206,7 @@ def run_ours(args):
         torch.cuda.set_device(local)
     dev = torch.device("cuda", local if ws > 1 else 0)
     mech, y, var = workload(args.num, args.seed, rank)
-    lu = A.LU_FP32 if args.lu == "fp32" else A.LU_FP64
+    lu = {"fp32": A.LU_FP32, "fp32_all": A.LU_FP32_ALL, "fp64": A.LU_FP64}[args.lu]
     integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu)
     stream = torch.cuda.Stream(device=dev)
     y0 = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
