@@ -18,8 +18,8 @@ ACCELERINT_ERR_UNSUPPORTED = -4
 ACCELERINT_ERR_SYSTEMS = -5
 SOLVERS = {"radau2a": 0, "exprb43": 1, "exp4": 2, "rkc": 3}
 LU_FP64, LU_FP32, LU_FP32_ALL = 0, 1, 2
-NSTATS = 8
-STAT_NAMES = ["steps", "accept", "reject", "jac", "decomp", "newton", "rhs", "aux"]
+NSTATS = 10
+STAT_NAMES = ["steps", "accept", "reject", "jac", "decomp", "newton", "rhs", "aux", "krylov", "arnoldi"]
 
 # Every symbol include/accelerint_b200.h declares.
 EXPORTED_SYMBOLS = [
@@ -28,7 +28,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_set_mechanism_mass_action", "accelerInt_set_tolerances",
     "accelerInt_set_lu_precision", "accelerInt_integrate_status", "accelerInt_integrate_device",
     "accelerInt_last_status", "accelerInt_get_codes", "accelerInt_get_poles", "accelerInt_version",
-    "accelerInt_measure_fma_peak", "accelerInt_integrate_device_noalloc",
+    "accelerInt_measure_fma_peak", "accelerInt_integrate_device_noalloc", "accelerInt_kernel_launches",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -57,6 +57,8 @@ def load_library():
     lib.accelerInt_cleanup.argtypes = []
     lib.accelerInt_cleanup.restype = None
     lib.accelerInt_set_solver.argtypes = [ctypes.c_int]
+    lib.accelerInt_kernel_launches.argtypes = []
+    lib.accelerInt_kernel_launches.restype = ctypes.c_longlong
     lib.accelerInt_set_mechanism_van_der_pol.argtypes = []
     lib.accelerInt_set_mechanism_mass_action.argtypes = [ctypes.POINTER(MassActionDesc)]
     lib.accelerInt_set_tolerances.argtypes = [ctypes.c_double, ctypes.c_double]
@@ -130,6 +132,10 @@ class Integrator:
             num, t_start, t_end, stepsize, y_dev.data_ptr(), var_dev.data_ptr(),
             codes_dev.data_ptr() if codes_dev is not None else None,
             stats_dev.data_ptr() if stats_dev is not None else None, s))
+
+    def kernel_launches(self) -> int:
+        """Kernels the library has launched in this process (all entry points)."""
+        return int(self.lib.accelerInt_kernel_launches())
 
     def poles(self):
         a = [np.zeros(10) for _ in range(4)]

@@ -16,7 +16,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
-SOURCES = ["api.cu"]
+SOURCES = ["api.cu", "cf.cpp"]
 
 
 def _nvcc():
@@ -39,7 +39,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     objs = []
     for src in SOURCES:
-        obj = os.path.join(CSRC, "_build", src.replace(".cu", ".o"))
+        obj = os.path.join(CSRC, "_build", os.path.splitext(src)[0] + ".o")
         os.makedirs(os.path.dirname(obj), exist_ok=True)
         cmd = [_nvcc()] + NVCC_FLAGS + ["-I", INCLUDE, "-c", os.path.join(CSRC, src), "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)

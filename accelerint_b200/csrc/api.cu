@@ -12,6 +12,10 @@
 
 using namespace aib;
 
+namespace aib_cf {
+int poles_residues(int n, double atol, double* pr, double* pi, double* rr, double* ri);
+}
+
 namespace {
 
 // FMA throughput probe: 8 independent dependency chains per thread.
@@ -59,6 +63,9 @@ struct State {
     int last_status = ACCELERINT_OK;
     std::vector<int> codes;
     double poles[4][10] = {};
+    double poles_atol = -1.0;     // ATOL the poles were computed for (< 0: not yet)
+    int poles_device = -1;        // device whose c_cf holds them
+    long long launches = 0;       // kernels this library launched
 };
 
 State g;
@@ -82,6 +89,33 @@ int ensure_jac(size_t doubles) {
     g.jac_doubles = 0;
     CK(cudaMalloc(&g.jac, doubles * sizeof(double)));
     g.jac_doubles = doubles;
+    return ACCELERINT_OK;
+}
+
+// CF poles and residues of the (10, 10) approximant for the current ATOL
+// (rational_approximant.c:23-44 computes them once at start-up).
+int compute_poles() {
+    if (g.poles_atol == g.atol) return ACCELERINT_OK;
+    if (aib_cf::poles_residues(CF_NRA, g.atol, g.poles[0], g.poles[1], g.poles[2], g.poles[3]) != 0)
+        return ACCELERINT_ERR_UNSUPPORTED;
+    g.poles_atol = g.atol;
+    g.poles_device = -1;
+    return ACCELERINT_OK;
+}
+
+int upload_poles() {
+    int rc = compute_poles();
+    if (rc) return rc;
+    if (g.poles_device == g.device) return ACCELERINT_OK;
+    CfTable tb;
+    for (int i = 0; i < CF_NRA; ++i) {
+        tb.pr[i] = g.poles[0][i];
+        tb.pi[i] = g.poles[1][i];
+        tb.rr[i] = g.poles[2][i];
+        tb.ri[i] = g.poles[3][i];
+    }
+    CK(cudaMemcpyToSymbol(c_cf, &tb, sizeof(tb)));
+    g.poles_device = g.device;
     return ACCELERINT_OK;
 }
 
@@ -148,7 +182,22 @@ int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
     CK(cudaMemsetAsync(a.queue, 0, sizeof(int), s));
     kern<<<grid, block, smem, s>>>(a, mech, lay);
     CK(cudaGetLastError());
+    g.launches++;
     return ACCELERINT_OK;
+}
+
+// EXPRB43 (P = 4) or EXP4 (P = 1) on block teams of TS threads.
+template <class Mech, int TS>
+int launch_krylov(BatchArgs a, const Mech& mech, int rhs_doubles, int jac_doubles, cudaStream_t s) {
+    constexpr int N = Mech::N;
+    int rc = upload_poles();
+    if (rc) return rc;
+    if (g.solver == ACCELERINT_EXPRB43) {
+        TeamLayout lay = TeamLayout::krylov(N, 4, rhs_doubles, jac_doubles);
+        return launch_team<SK_EXPRB43, Mech, TS, double>(a, mech, lay, s);
+    }
+    TeamLayout lay = TeamLayout::krylov(N, 1, rhs_doubles, jac_doubles);
+    return launch_team<SK_EXP4, Mech, TS, double>(a, mech, lay, s);
 }
 
 template <int K, int TS>
@@ -173,6 +222,8 @@ int launch_mass_action(BatchArgs a, cudaStream_t s) {
         TeamLayout lay = TeamLayout::rkc(N, M::smem_rhs(R));
         return launch_team<SK_RKC, M, TS, double>(a, mech, lay, s);
     }
+    if (g.solver == ACCELERINT_EXPRB43 || g.solver == ACCELERINT_EXP4)
+        return launch_krylov<M, TS>(a, mech, M::smem_rhs(R), M::smem_jac(R), s);
     return ACCELERINT_ERR_UNSUPPORTED;
 }
 
@@ -183,10 +234,13 @@ int launch_vdp(BatchArgs a, cudaStream_t s) {
         else tps_kernel<SK_RADAU, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
     } else if (g.solver == ACCELERINT_RKC) {
         tps_kernel<SK_RKC, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
+    } else if (g.solver == ACCELERINT_EXPRB43 || g.solver == ACCELERINT_EXP4) {
+        return launch_krylov<VanDerPol, 32>(a, VanDerPol{}, 0, 0, s);
     } else {
         return ACCELERINT_ERR_UNSUPPORTED;
     }
     CK(cudaGetLastError());
+    g.launches++;
     return ACCELERINT_OK;
 }
 
@@ -409,6 +463,8 @@ int accelerInt_get_codes(int* codes_host, int NUM) {
 
 int accelerInt_get_poles(double* pr, double* pi, double* rr, double* ri) {
     if (!pr || !pi || !rr || !ri) return ACCELERINT_ERR_ARGUMENT;
+    const int rc = compute_poles();
+    if (rc) return rc;
     for (int i = 0; i < 10; ++i) {
         pr[i] = g.poles[0][i];
         pi[i] = g.poles[1][i];
@@ -417,6 +473,8 @@ int accelerInt_get_poles(double* pr, double* pi, double* rr, double* ri) {
     }
     return ACCELERINT_OK;
 }
+
+long long accelerInt_kernel_launches(void) { return g.launches; }
 
 const char* accelerInt_version(void) { return "accelerint_b200 0.1 (sm_100a)"; }
 
@@ -512,6 +570,7 @@ int launch_team_noalloc(BatchArgs a, const Mech& mech, TeamLayout lay, unsigned 
     CK(cudaMemsetAsync(a.queue, 0, sizeof(int), s));   // the counter must start at zero on every call
     kern<<<grid, block, smem, s>>>(a, mech, lay);
     CK(cudaGetLastError());
+    g.launches++;
     return ACCELERINT_OK;
 }
 

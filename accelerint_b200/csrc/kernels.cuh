@@ -16,6 +16,7 @@
 #include "mech.cuh"
 #include "radau2a.cuh"
 #include "rkc.cuh"
+#include "krylov.cuh"
 
 namespace aib {
 
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(128) tps_kernel(BatchArgs a, Mech mech)
 // Shared-memory layout of one team (bytes, 16-byte aligned pieces).
 struct TeamLayout {
     int e1, e2, d1, d2, p1, p2, buf, rhs, inf, total;
+    int vm, hm, phi, inv, cw, piv, mv, nv;   // Krylov methods
     __host__ __device__ static int al(int b) { return (b + 15) & ~15; }
     // lt_bytes: element size of E2's real type; l1_bytes: of E1
     __host__ __device__ static TeamLayout radau(int N, int lt_bytes, int rhs_doubles, int jac_doubles,
@@ -115,6 +117,26 @@ struct TeamLayout {
         L.buf = o; o += al(3 * N * 8);
         L.rhs = o; o += al(rhs_doubles * 8);
         L.inf = o; o += al(2 * 4);
+        L.total = o;
+        return L;
+    }
+    // stride = N + P; the complex work matrix doubles as mechanism scratch
+    __host__ __device__ static TeamLayout krylov(int N, int P, int rhs_doubles, int jac_doubles) {
+        TeamLayout L{};
+        const int S = N + P;
+        int o = 0;
+        L.vm = o; o += al(N * S * 8);
+        L.hm = o; o += al(S * S * 8);
+        L.phi = o; o += al(S * S * 8);
+        L.inv = o;
+        int ib = S * S * 16;
+        if (rhs_doubles * 8 > ib) ib = rhs_doubles * 8;
+        if (jac_doubles * 8 > ib) ib = jac_doubles * 8;
+        o += al(ib);
+        L.cw = o; o += al(S * 16);
+        L.piv = o; o += al(S * 4);
+        L.mv = o; o += al(2 * S * 8);
+        L.nv = o; o += al(N * 8);
         L.total = o;
         return L;
     }
@@ -174,6 +196,25 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             Rkc<N, TS, Mech> rk{mech, reinterpret_cast<double*>(base + lay.rhs), a.atol, a.rtol, pr, st};
             while (L.more() && code == EC_success) {
                 code = rk.integrate(L.t, L.t_next, y);
+                L.advance();
+            }
+        } else if constexpr (SK == SK_EXPRB43 || SK == SK_EXP4) {
+            constexpr int P = SK == SK_EXPRB43 ? 4 : 1;
+            KrylovStore ks;
+            ks.J = a.jac + size_t(gteam) * N * N;
+            ks.Vm = reinterpret_cast<double*>(base + lay.vm);
+            ks.Hm = reinterpret_cast<double*>(base + lay.hm);
+            ks.phiHm = reinterpret_cast<double*>(base + lay.phi);
+            ks.inv = reinterpret_cast<cxd*>(base + lay.inv);
+            ks.cw = reinterpret_cast<cxd*>(base + lay.cw);
+            ks.piv = reinterpret_cast<int*>(base + lay.piv);
+            ks.mv0 = reinterpret_cast<double*>(base + lay.mv);
+            ks.mv1 = ks.mv0 + (N + P);
+            ks.nv = reinterpret_cast<double*>(base + lay.nv);
+            Krylov<N, TS, Mech, P> kr{mech, ks, a.atol, a.rtol, pr, st};
+            while (L.more() && code == EC_success) {
+                if constexpr (SK == SK_EXPRB43) code = kr.integrate_exprb43(L.t, L.t_next, y);
+                else code = kr.integrate_exp4(L.t, L.t_next, y);
                 L.advance();
             }
         }

@@ -19,17 +19,35 @@ struct VanDerPol {
     static constexpr int N = 2;
     static constexpr int SMEM_RHS = 0;
     static constexpr int SMEM_JAC = 0;
+    // TS = 1: the thread owns both elements.  TS > 1 (a team): lane 0 owns y1 and
+    // lane 1 owns y2; the Jacobian is written by lane 0.
     template <int TS>
-    __device__ __forceinline__ void dydt(double, double mu, const Vec<2, 1>& y, Vec<2, 1>& dy, double*) const {
-        dy[0] = y[1];
-        dy[1] = mu * (1 - y[0] * y[0]) * y[1] - y[0];
+    __device__ __forceinline__ void dydt(double, double mu, const Vec<2, TS>& y, Vec<2, TS>& dy, double*) const {
+        if constexpr (TS == 1) {
+            dy[0] = y[1];
+            dy[1] = mu * (1 - y[0] * y[0]) * y[1] - y[0];
+        } else {
+            const double y0 = Team<TS>::bcast(y[0], 0), y1 = Team<TS>::bcast(y[0], 1);
+            const int l = Team<TS>::lane();
+            dy[0] = l == 0 ? y1 : (l == 1 ? mu * (1 - y0 * y0) * y1 - y0 : 0.0);
+        }
     }
     template <int TS>
-    __device__ __forceinline__ void jacob(double, double mu, const Vec<2, 1>& y, double* jac, double*) const {
-        jac[0] = 0;
-        jac[1] = -2 * mu * y[0] * y[1] - 1;
-        jac[2] = 1;
-        jac[3] = mu * (1 - y[0] * y[0]);
+    __device__ __forceinline__ void jacob(double, double mu, const Vec<2, TS>& y, double* jac, double*) const {
+        double y0, y1;
+        if constexpr (TS == 1) {
+            y0 = y[0];
+            y1 = y[1];
+        } else {
+            y0 = Team<TS>::bcast(y[0], 0);
+            y1 = Team<TS>::bcast(y[0], 1);
+        }
+        if (Team<TS>::lane() == 0) {
+            jac[0] = 0;
+            jac[1] = -2 * mu * y0 * y1 - 1;
+            jac[2] = 1;
+            jac[3] = mu * (1 - y0 * y0);
+        }
     }
 };
 

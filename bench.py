@@ -1,14 +1,20 @@
 #!/usr/bin/env python
 """Throughput benchmark: ODE systems/s per global Delta-t step.
 
-Workload (default): the 53-species / 325-reaction synthetic mechanism, 1,048,576
-initial conditions (half near equilibrium at 800-1200 K, half ignition at
-1400-2400 K, interleaved), Radau IIA at rtol 1e-6 / atol 1e-10, global steps of
-dt = 1e-6 s from t = 0.  A bench step is one global Delta-t step of all
-systems; the timed region runs K consecutive global steps starting from the
-initial conditions (the warm-up runs W steps from the same initial conditions,
-then the state is reset), so the transient after t = 0 is always inside the
-timed region.
+Workload (default): the 53-species / 325-reaction synthetic mechanism, 65,536
+initial conditions of the mixed-stiffness generator (half near equilibrium at
+800-1200 K, half ignition at 1400-2400 K, interleaved), Radau IIA at rtol 1e-6 /
+atol 1e-10, global steps of dt = 1e-6 s from t = 0.  The 1,048,576-IC batch is
+`--num 1048576`; one global step of it takes minutes, so the default run uses a
+65,536-IC batch from the same generator.  A bench step is one global Delta-t
+step of all systems; the timed region runs K consecutive global steps starting
+from the initial conditions (the warm-up runs W steps from the same initial
+conditions, then the state is reset), so the transient after t = 0 is always
+inside the timed region.  L2 is flushed (a 256 MiB write) between timed steps,
+outside the per-step event pairs.
+
+Beside the tuned form (LU in FP32, the default) the plain FP64 form is timed on
+the same batch for `--plain-steps` global steps and reported as "plain_fp64".
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--lu fp32|fp64] [--num NUM] [--solver radau2a]
@@ -44,14 +50,19 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--lu", default="fp32", choices=["fp32", "fp32_all", "fp64"])
-    p.add_argument("--num", type=int, default=1 << 20)
+    p.add_argument("--lu", default="fp32_all", choices=["fp32", "fp32_all", "fp64"])
+    p.add_argument("--plain-steps", type=int, default=-1,
+                   help="global steps of the plain FP64 comparison (-1: as --steps, 0: skip)")
+    p.add_argument("--num", type=int, default=1 << 16)
     p.add_argument("--solver", default="radau2a")
     p.add_argument("--seed", type=int, default=2024)
     p.add_argument("--cpu-sample", type=int, default=0, help="systems in the CPU baseline sample (0: auto)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    return p.parse_args()
+    args = p.parse_args()
+    if args.plain_steps < 0:
+        args.plain_steps = args.steps
+    return args
 
 
 def dist_env():
@@ -149,7 +160,9 @@ def cpu_baseline(args, mech, y, var):
     sys.path.insert(0, ROOT)
     from oracle import Reference, reference_available, Oracle, oracle_available
     nthreads = os.cpu_count() or 1
-    sample = args.cpu_sample or 512
+    # ~8 systems per thread: one 53-species global step costs ~0.36 s per system on one
+    # core, so K = 3 steps of the sample take ~10 s whatever the core count
+    sample = args.cpu_sample or min(args.num, 4096, 8 * nthreads)
     ys, vs = y[:, :sample].copy(), var[:sample].copy()
     if reference_available("radau2a", 54):
         ref = Reference("radau2a", 54)
@@ -227,19 +240,20 @@ def run_ours(args):
             integ.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, codes, None, stream)
         yd.copy_(y0)
     barrier()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    launches = 0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = integ.kernel_launches()
     with ClockSampler(dev.index) as clk:
         barrier()
         with torch.cuda.stream(stream):
-            ev0.record(stream)
             for k in range(args.steps):
+                flush.fill_(k & 0xff)
+                evs[k][0].record(stream)
                 integ.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, codes, stats, stream)
-                launches += 1
-            ev1.record(stream)
+                evs[k][1].record(stream)
         barrier()
-    ms = ev0.elapsed_time(ev1)
+    launches = integ.kernel_launches() - launches0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
     t_max = ms
     if ws > 1:
         import torch.distributed as dist
@@ -268,21 +282,53 @@ def run_ours(args):
         nb = args.num * (mech.n_state + 1) * 8
         e2e = {"value": ws * args.num * args.steps / el, "unit": UNIT,
                "h2d_bytes_per_step": nb, "d2h_bytes_per_step": args.num * mech.n_state * 8 + args.num * 4}
-    line = None
+    integ.close()
+
+    # the plain FP64 form on the same batch, for the tuned-vs-plain ratio
+    plain = None
+    if args.plain_steps > 0 and args.lu != "fp64":
+        pinteg = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=A.LU_FP64)
+        nw = min(args.num, 4 * 148)
+        yw = y0[:, :nw].contiguous()
+        pinteg.integrate_device(0.0, DT, DT, yw, vd[:nw].contiguous(), None, None, stream)   # warm-up
+        yd.copy_(y0)
+        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.plain_steps)]
+        barrier()
+        with torch.cuda.stream(stream):
+            for k in range(args.plain_steps):
+                flush.fill_(k & 0xff)
+                pev[k][0].record(stream)
+                pinteg.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, None, None, stream)
+                pev[k][1].record(stream)
+        barrier()
+        pms = sum(a.elapsed_time(b) for a, b in pev)
+        if ws > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([pms], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            pms = float(tt.item())
+        pinteg.close()
+        pval = ws * args.num * args.plain_steps / (pms / 1000.0)
+        plain = {"value": pval, "unit": UNIT, "ms_per_step": pms / args.plain_steps, "steps": args.plain_steps,
+                 "tuned_over_plain": value / pval}
+
     if rank == 0:
         cb = None if args.no_cpu_baseline else cpu_baseline(args, mech, y, var)
+        mb = args.num * mech.n_state * 8 / 1e6
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.lu == "fp64" else "f64 (E1/E2 factorised and solved in f32)",
+                "data": "synthetic",
                 "config": {"workload": f"mass-action 53 species / 325 reactions, mixed stiffness, {args.num} ICs "
                                        f"per GPU, global steps of dt=1e-6 s from t=0, {args.solver} rtol 1e-6 "
                                        f"atol 1e-10, LU {args.lu}, persistent work-queue team kernel",
-                           "l2": "inputs (y: 432 MB per GPU) larger than L2; no flush",
+                           "l2": f"L2 flushed (256 MiB write) before every timed step; state y is {mb:.0f} MB",
                            "failed_systems": nfail},
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cb}
+                "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain}
         print(json.dumps(line))
-    integ.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

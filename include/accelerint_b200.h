@@ -106,7 +106,7 @@ int accelerInt_integrate_status(int NUM, double t_start, double t_end, double st
  * system, stats_dev[ivp * ACCELERINT_NSTATS + k], added to what the array holds
  * (zero it before the first call).  Asynchronous on `stream`
  * (a cudaStream_t, NULL = the legacy default stream). */
-#define ACCELERINT_NSTATS 8   /* steps, accept, reject, jac, decomp, newton, rhs, errsolve/krylov */
+#define ACCELERINT_NSTATS 10  /* steps, accept, reject, jac, decomp, newton, rhs, errsolve, krylov dims, arnoldi calls */
 int accelerInt_integrate_device(int NUM, double t_start, double t_end, double stepsize,
                                 double* y_dev, const double* var_dev, int* codes_dev,
                                 int* stats_dev, void* stream);
@@ -135,8 +135,13 @@ int accelerInt_integrate_device_noalloc(int NUM, double t_start, double t_end, d
 int accelerInt_last_status(void);
 /* Copies the EC_* codes of the last accelerInt_integrate* call (host pointer, NUM entries). */
 int accelerInt_get_codes(int* codes_host, int NUM);
-/* Poles and residues of the (10,10) rational approximant in use (exp methods). */
+/* Poles and residues of the (10,10) Caratheodory-Fejer approximant of exp on
+ * (-inf, 0] that the exp methods use, computed on the host for the current ATOL
+ * (exponential_integrators/rational_approximant.c:23-44, cf.c:41-312); no GPU
+ * needed.  Conjugate pairs, positive imaginary part first. */
 int accelerInt_get_poles(double* poles_re, double* poles_im, double* res_re, double* res_im);
+/* Extension: number of kernels this library has launched in the process. */
+long long accelerInt_kernel_launches(void);
 const char* accelerInt_version(void);
 
 /* Diagnostic: measured FMA throughput of the current device in TFLOP/s (FMA = 2

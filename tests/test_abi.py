@@ -39,3 +39,29 @@ def test_setters_validate_without_a_device():
     assert lib.accelerInt_set_solver(99) == -1
     assert lib.accelerInt_set_tolerances(-1.0, 1e-6) == -1
     assert lib.accelerInt_set_lu_precision(7) == -1
+
+
+def test_host_cf_poles_match_reference():
+    """accelerInt_get_poles runs the library's own C++ CF solver on the host (no GPU):
+    its poles and residues match the reference's cf() output stored with the fixtures
+    (to the conditioning of the Hankel SVD and the polynomial roots), in the same
+    conjugate-pair order."""
+    import ctypes
+    import numpy as np
+    lib = _lib()
+    lib.accelerInt_set_tolerances(1e-10, 1e-6)
+    a = [np.zeros(10) for _ in range(4)]
+    dp = ctypes.POINTER(ctypes.c_double)
+    assert lib.accelerInt_get_poles(*[x.ctypes.data_as(dp) for x in a]) == 0
+    p, r = a[0] + 1j * a[1], a[2] + 1j * a[3]
+    g = np.load(os.path.join(ROOT, "tests", "golden", "vdp_exprb43.npz"))
+    assert np.max(np.abs(p - g["poles"]) / np.abs(g["poles"])) < 1e-7
+    assert np.max(np.abs(r - g["res"]) / np.abs(g["res"])) < 1e-6
+    assert np.allclose(p[0::2], np.conj(p[1::2]), rtol=0, atol=0)
+
+
+def test_kernel_launch_counter_is_exported():
+    import ctypes
+    lib = _lib()
+    lib.accelerInt_kernel_launches.restype = ctypes.c_longlong
+    assert lib.accelerInt_kernel_launches() >= 0
