@@ -29,6 +29,9 @@ EXPORTED_SYMBOLS = [
     "accelerInt_set_lu_precision", "accelerInt_integrate_status", "accelerInt_integrate_device",
     "accelerInt_last_status", "accelerInt_get_codes", "accelerInt_get_poles", "accelerInt_version",
     "accelerInt_measure_fma_peak", "accelerInt_integrate_device_noalloc", "accelerInt_kernel_launches",
+    "accelerInt_mlp_sizes", "accelerInt_mlp_forward", "accelerInt_mlp_loss_grad", "accelerInt_mlp_adam_step",
+    "accelerInt_set_learned", "accelerInt_set_step_recording", "accelerInt_set_graph_launch",
+    "accelerInt_set_launch_config", "accelerInt_autotune",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -57,6 +60,16 @@ def load_library():
     lib.accelerInt_cleanup.argtypes = []
     lib.accelerInt_cleanup.restype = None
     lib.accelerInt_set_solver.argtypes = [ctypes.c_int]
+    vp, i, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    lib.accelerInt_mlp_sizes.argtypes = [vp, vp, vp, vp]
+    lib.accelerInt_mlp_forward.argtypes = [vp, vp, vp, i, vp, vp]
+    lib.accelerInt_mlp_loss_grad.argtypes = [vp, vp, vp, vp, i, vp, vp, vp]
+    lib.accelerInt_mlp_adam_step.argtypes = [vp, vp, vp, vp, i, f, f, f, f, vp]
+    lib.accelerInt_set_learned.argtypes = [vp, vp, i]
+    lib.accelerInt_set_step_recording.argtypes = [vp, vp, i]
+    lib.accelerInt_set_graph_launch.argtypes = [i]
+    lib.accelerInt_set_launch_config.argtypes = [i, i]
+    lib.accelerInt_autotune.argtypes = [i, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, i, vp, vp, vp]
     lib.accelerInt_kernel_launches.argtypes = []
     lib.accelerInt_kernel_launches.restype = ctypes.c_longlong
     lib.accelerInt_set_mechanism_van_der_pol.argtypes = []
@@ -132,6 +145,18 @@ class Integrator:
             num, t_start, t_end, stepsize, y_dev.data_ptr(), var_dev.data_ptr(),
             codes_dev.data_ptr() if codes_dev is not None else None,
             stats_dev.data_ptr() if stats_dev is not None else None, s))
+
+    def autotune(self, t_start, t_end, stepsize, y_dev, var_dev, sample: int):
+        """Pick the launch mapping by timing candidates on a copy of the first `sample` systems.
+        Returns (occupancy cap, thread-per-system block size, best ms)."""
+        occ, blk, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.accelerInt_autotune(y_dev.shape[1], t_start, t_end, stepsize, y_dev.data_ptr(),
+                                                 var_dev.data_ptr(), int(sample), ctypes.byref(occ),
+                                                 ctypes.byref(blk), ctypes.byref(ms)))
+        return occ.value, blk.value, ms.value
+
+    def set_graph_launch(self, enable: bool = True):
+        self._check(self.lib.accelerInt_set_graph_launch(1 if enable else 0))
 
     def kernel_launches(self) -> int:
         """Kernels the library has launched in this process (all entry points)."""

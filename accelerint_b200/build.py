@@ -16,7 +16,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
-SOURCES = ["api.cu", "cf.cpp"]
+SOURCES = ["api.cu", "mlp.cu", "cf.cpp"]
 
 
 def _nvcc():

@@ -15,6 +15,9 @@ using namespace aib;
 namespace aib_cf {
 int poles_residues(int n, double atol, double* pr, double* pi, double* rr, double* ri);
 }
+namespace aib_mlp {
+int to_bf16(const float* params, void* w_bf16, cudaStream_t s);
+}
 
 namespace {
 
@@ -66,6 +69,16 @@ struct State {
     double poles_atol = -1.0;     // ATOL the poles were computed for (< 0: not yet)
     int poles_device = -1;        // device whose c_cf holds them
     long long launches = 0;       // kernels this library launched
+    LearnArgs learn{};            // learned proposals / step records for the Radau block teams
+    void* mlp_w = nullptr;        // bf16 weight copy of the installed model
+    // launch mapping (autotuned): resident blocks per SM cap (0: occupancy maximum)
+    // for the persistent team kernels, block size of the thread-per-system kernels
+    int occ_cap = 0;
+    int tps_block = 128;
+    int last_occ = 0;             // resident blocks per SM of the last team launch
+    bool graph = false;           // device-buffer launches through a captured CUDA graph
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t cap_stream = nullptr;
 };
 
 State g;
@@ -162,17 +175,19 @@ template <class K> int persistent_grid(K kernel, int block, size_t smem, int num
     int nb = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, smem));
     if (nb <= 0) return ACCELERINT_ERR_UNSUPPORTED;
+    if (g.occ_cap > 0) nb = std::min(nb, g.occ_cap);
+    g.last_occ = nb;
     const int need = (num_teams_needed + teams_per_block - 1) / teams_per_block;
     *grid = std::max(1, std::min(nb * g.num_sms, need));
     return ACCELERINT_OK;
 }
 
-template <int SK, class Mech, int TS, typename LT, typename L1 = LT>
+template <int SK, class Mech, int TS, typename LT, typename L1 = LT, bool LEARN = false>
 int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
     constexpr int N = Mech::N;
     const int block = TS >= 32 ? TS : 32, tpb = block / TS;
     const size_t smem = size_t(lay.total) * tpb;
-    auto kern = team_kernel<SK, Mech, TS, LT, L1>;
+    auto kern = team_kernel<SK, Mech, TS, LT, L1, LEARN>;
     int grid = 0;
     int rc = persistent_grid(kern, block, smem, a.num, tpb, &grid);
     if (rc) return rc;
@@ -207,15 +222,19 @@ int launch_mass_action(BatchArgs a, cudaStream_t s) {
     const int R = g.mt.R;
     constexpr int N = M::N;
     if (g.solver == ACCELERINT_RADAU2A) {
+        const bool learn = a.learn.rec != nullptr || a.learn.mlp.flags != 0;
         if (g.lu == ACCELERINT_LU_FP32) {
             TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 8);
+            if (learn) return launch_team<SK_RADAU, M, TS, float, double, true>(a, mech, lay, s);
             return launch_team<SK_RADAU, M, TS, float, double>(a, mech, lay, s);
         }
         if (g.lu == ACCELERINT_LU_FP32_ALL) {
             TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 4);
+            if (learn) return launch_team<SK_RADAU, M, TS, float, float, true>(a, mech, lay, s);
             return launch_team<SK_RADAU, M, TS, float, float>(a, mech, lay, s);
         }
         TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
+        if (learn) return launch_team<SK_RADAU, M, TS, double, double, true>(a, mech, lay, s);
         return launch_team<SK_RADAU, M, TS, double>(a, mech, lay, s);
     }
     if (g.solver == ACCELERINT_RKC) {
@@ -228,7 +247,7 @@ int launch_mass_action(BatchArgs a, cudaStream_t s) {
 }
 
 int launch_vdp(BatchArgs a, cudaStream_t s) {
-    const int block = 128, grid = (a.num + block - 1) / block;
+    const int block = g.tps_block, grid = (a.num + block - 1) / block;
     if (g.solver == ACCELERINT_RADAU2A) {
         if (g.lu == ACCELERINT_LU_FP32) tps_kernel<SK_RADAU, VanDerPol, float><<<grid, block, 0, s>>>(a, VanDerPol{});
         else tps_kernel<SK_RADAU, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
@@ -278,6 +297,7 @@ int run_chunked(int NUM, double t_start, double t_end, double stepsize, double* 
         a.queue = g.queue;
         a.atol = g.atol;
         a.rtol = g.rtol;
+        a.learn = g.learn;
         int rc = launch(a, s);
         if (rc) return rc;
         CK(cudaMemcpy2DAsync(y_host + off, size_t(NUM) * sizeof(double), g.y_dev, cnt * sizeof(double),
@@ -287,6 +307,42 @@ int run_chunked(int NUM, double t_start, double t_end, double stepsize, double* 
     }
     for (int c : g.codes)
         if (c != 0) return ACCELERINT_ERR_SYSTEMS;
+    return ACCELERINT_OK;
+}
+
+// Record this call's launch sequence (queue reset + kernel) by stream capture,
+// update the cached executable graph in place when only parameters changed,
+// and launch it on the caller's stream.
+int launch_graph(BatchArgs a, cudaStream_t s) {
+    if (!g.cap_stream) CK(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(g.cap_stream, cudaStreamCaptureModeRelaxed));
+    const int rc = launch(a, g.cap_stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(g.cap_stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    CK(ec);
+    bool updated = false;
+    if (g.gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(g.gexec, graph, &info) == cudaSuccess;
+        if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(g.gexec);
+            g.gexec = nullptr;
+        }
+    }
+    if (!updated) {
+        const cudaError_t ei = cudaGraphInstantiate(&g.gexec, graph, 0);
+        if (ei != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            CK(ei);
+        }
+    }
+    cudaGraphDestroy(graph);
+    CK(cudaGraphLaunch(g.gexec, s));
     return ACCELERINT_OK;
 }
 
@@ -346,6 +402,15 @@ void accelerInt_cleanup(void) {
     if (g.codes_dev) cudaFree(g.codes_dev);
     if (g.jac) cudaFree(g.jac);
     if (g.queue) cudaFree(g.queue);
+    if (g.mlp_w) cudaFree(g.mlp_w);
+    g.mlp_w = nullptr;
+    if (g.gexec) cudaGraphExecDestroy(g.gexec);
+    g.gexec = nullptr;
+    if (g.cap_stream) cudaStreamDestroy(g.cap_stream);
+    g.cap_stream = nullptr;
+    g.occ_cap = 0;
+    g.tps_block = 128;
+    g.learn = LearnArgs{};
     if (g.dev_tb_mem) cudaFree(g.dev_tb_mem);
     if (g.stream) cudaStreamDestroy(g.stream);
     g.y_dev = nullptr;
@@ -450,7 +515,13 @@ int accelerInt_integrate_device(int NUM, double t_start, double t_end, double st
     a.queue = g.queue;
     a.atol = g.atol;
     a.rtol = g.rtol;
-    return launch(a, static_cast<cudaStream_t>(stream));
+    a.learn = g.learn;
+    if (!g.graph) return launch(a, static_cast<cudaStream_t>(stream));
+    if (g.solver == ACCELERINT_EXPRB43 || g.solver == ACCELERINT_EXP4) {
+        const int rc = upload_poles();   // a synchronous copy: before the capture
+        if (rc) return rc;
+    }
+    return launch_graph(a, static_cast<cudaStream_t>(stream));
 }
 
 int accelerInt_last_status(void) { return g.last_status; }
@@ -475,6 +546,119 @@ int accelerInt_get_poles(double* pr, double* pi, double* rr, double* ri) {
 }
 
 long long accelerInt_kernel_launches(void) { return g.launches; }
+
+int accelerInt_set_learned(const float* params_dev, const float* norm_dev, int flags) {
+    if (flags & ~(ACCELERINT_MLP_USE_H | ACCELERINT_MLP_USE_Z)) return ACCELERINT_ERR_ARGUMENT;
+    if (flags == 0) {
+        g.learn.mlp = MlpDevice{};
+        return ACCELERINT_OK;
+    }
+    if (!params_dev || !norm_dev) return ACCELERINT_ERR_ARGUMENT;
+    if (!g.initialized) return ACCELERINT_ERR_STATE;
+    if (!g.mlp_w) CK(cudaMalloc(&g.mlp_w, size_t(MLP_NWEIGHT) * 2));
+    if (aib_mlp::to_bf16(params_dev, g.mlp_w, nullptr)) return ACCELERINT_ERR_CUDA;
+    CK(cudaDeviceSynchronize());
+    g.learn.mlp.w = static_cast<const __nv_bfloat16*>(g.mlp_w);
+    g.learn.mlp.p = params_dev;
+    g.learn.mlp.norm = norm_dev;
+    g.learn.mlp.flags = flags;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_graph_launch(int enable) {
+    g.graph = enable != 0;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_launch_config(int occupancy_cap, int tps_block) {
+    if (occupancy_cap < 0 || (tps_block != 0 && (tps_block < 32 || tps_block > 1024 || tps_block % 32)))
+        return ACCELERINT_ERR_ARGUMENT;
+    g.occ_cap = occupancy_cap;
+    if (tps_block) g.tps_block = tps_block;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, const double* y_dev,
+                        const double* var_dev, int sample, int* occupancy_cap_out, int* tps_block_out,
+                        double* best_ms_out) {
+    if (!g.initialized) return ACCELERINT_ERR_STATE;
+    if (NUM <= 0 || !y_dev || !var_dev || sample <= 0) return ACCELERINT_ERR_ARGUMENT;
+    sample = std::min(sample, NUM);
+    const int N = state_n();
+    double* ys = nullptr;
+    CK(cudaMalloc(&ys, size_t(sample) * N * sizeof(double)));
+    cudaStream_t s = g.stream;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto trial = [&](double* ms) -> int {
+        CK(cudaMemcpy2DAsync(ys, sample * sizeof(double), y_dev, size_t(NUM) * sizeof(double),
+                             sample * sizeof(double), N, cudaMemcpyDeviceToDevice, s));
+        BatchArgs a{};
+        a.num = sample;
+        a.t_start = t_start;
+        a.t_end = t_end;
+        a.step = stepsize < 0 ? t_end - t_start : stepsize;
+        a.y = ys;
+        a.var = var_dev;
+        a.queue = g.queue;
+        a.atol = g.atol;
+        a.rtol = g.rtol;
+        a.learn = g.learn;
+        CK(cudaEventRecord(e0, s));
+        int rc = launch(a, s);
+        if (rc) return rc;
+        CK(cudaEventRecord(e1, s));
+        CK(cudaEventSynchronize(e1));
+        float f = 0;
+        CK(cudaEventElapsedTime(&f, e0, e1));
+        *ms = f;
+        return ACCELERINT_OK;
+    };
+    int rc = ACCELERINT_OK;
+    double best = 1e300, ms = 0;
+    if (g.mech_kind == 0 && (g.solver == ACCELERINT_RADAU2A || g.solver == ACCELERINT_RKC)) {
+        // thread per system: block size
+        int best_b = g.tps_block;
+        for (int b : {64, 128, 256, 512}) {
+            g.tps_block = b;
+            if ((rc = trial(&ms))) break;
+            if (ms < best) { best = ms; best_b = b; }
+        }
+        g.tps_block = best_b;
+    } else {
+        // persistent teams: resident blocks per SM, from the occupancy maximum down to half of it
+        g.occ_cap = 0;
+        rc = trial(&ms);   // also measures the maximum
+        int best_c = 0;
+        if (!rc) {
+            best = ms;
+            const int mx = g.last_occ;
+            for (int c = mx - 1; c >= std::max(1, (mx + 1) / 2) && !rc; --c) {
+                g.occ_cap = c;
+                if ((rc = trial(&ms))) break;
+                if (ms < best) { best = ms; best_c = c; }
+            }
+        }
+        g.occ_cap = best_c;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(ys);
+    if (rc) return rc;
+    if (occupancy_cap_out) *occupancy_cap_out = g.occ_cap;
+    if (tps_block_out) *tps_block_out = g.tps_block;
+    if (best_ms_out) *best_ms_out = best;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_step_recording(float* rec_dev, int* count_dev, int capacity) {
+    if (rec_dev && (!count_dev || capacity < 0)) return ACCELERINT_ERR_ARGUMENT;
+    g.learn.rec = rec_dev;
+    g.learn.rec_count = rec_dev ? count_dev : nullptr;
+    g.learn.rec_cap = rec_dev ? capacity : 0;
+    return ACCELERINT_OK;
+}
 
 const char* accelerInt_version(void) { return "accelerint_b200 0.1 (sm_100a)"; }
 

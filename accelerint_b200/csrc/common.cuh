@@ -20,8 +20,10 @@ enum : int {
 // Per-system counters (stats_dev[ivp * NSTATS + k]).
 enum : int {
     ST_STEPS = 0, ST_ACCEPT, ST_REJECT, ST_JAC, ST_DECOMP, ST_NEWTON, ST_RHS, ST_AUX,
-    ST_KRYLOV,    // exponential methods: sum of Krylov dimensions over Arnoldi calls
-    ST_ARNOLDI,   // exponential methods: Arnoldi calls
+    ST_KRYLOV,    // exponential methods: sum of Krylov dimensions over Arnoldi calls;
+                  // Radau in learned mode: steps started from a learned proposal
+    ST_ARNOLDI,   // exponential methods: Arnoldi calls;
+                  // Radau in learned mode: fall-backs to the extrapolated guess
     NSTATS
 };
 

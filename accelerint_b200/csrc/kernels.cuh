@@ -30,6 +30,7 @@ struct BatchArgs {
     int* queue;             // work-queue counter (zeroed before launch)
     double* jac;            // per-team Jacobian scratch [teams * N * N]
     double atol, rtol;
+    LearnArgs learn;        // Radau block teams: learned proposals / step records (zero: off)
 };
 
 // The reference's global-step loop (generic/solver_main.c:196-209), measured from t_start.
@@ -115,7 +116,9 @@ struct TeamLayout {
         L.p1 = o; o += al(N * 4);
         L.p2 = o; o += al(N * 4);
         L.buf = o; o += al(3 * N * 8);
-        L.rhs = o; o += al(rhs_doubles * 8);
+        // dydt scratch; also holds the MLP input and activations in learned mode
+        const int rb = rhs_doubles * 8 > (MLP_D0 + 2 * MLP_D4) * 4 ? rhs_doubles * 8 : (MLP_D0 + 2 * MLP_D4) * 4;
+        L.rhs = o; o += al(rb);
         L.inf = o; o += al(2 * 4);
         L.total = o;
         return L;
@@ -149,7 +152,7 @@ struct TeamLayout {
     }
 };
 
-template <int SK, class Mech, int TS, typename LT, typename L1 = LT>
+template <int SK, class Mech, int TS, typename LT, typename L1 = LT, bool LEARN = false>
 __global__ void __launch_bounds__(TS >= 32 ? TS : 32, (TS >= 64 && sizeof(L1) == 4) ? 5 : 1)
 team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
 {
@@ -187,7 +190,9 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             store.buf = reinterpret_cast<double*>(base + lay.buf);
             store.rhs = reinterpret_cast<double*>(base + lay.rhs);
             store.inf = reinterpret_cast<int*>(base + lay.inf);
-            Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
+            const LearnArgs la = a.learn;
+            Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>, LEARN> rad{mech, store, RadauParams{a.atol, a.rtol},
+                                                                         pr, st, LEARN ? &la : nullptr};
             while (L.more() && code == EC_success) {
                 code = rad.integrate(L.t, L.t_next, y);
                 L.advance();

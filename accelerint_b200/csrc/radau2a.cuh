@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "linalg.cuh"
 #include "wlinalg.cuh"
+#include "mlp.cuh"
 
 namespace aib {
 
@@ -128,10 +129,12 @@ struct RadauParams {
     double atol, rtol;
 };
 
-template <int N, int TS, class Mech, typename LT, class Store>
+// LEARN: learned proposals and step records compiled in (block teams only)
+template <int N, int TS, class Mech, typename LT, class Store, bool LEARN = false>
 struct Radau {
     using V = Vec<N, TS>;
     using TM = Team<TS>;
+    static_assert(!LEARN || TM::block, "learned mode runs on block teams");
     using L1 = typename Store::E1T;
     static constexpr int S = V::S;
 
@@ -140,6 +143,37 @@ struct Radau {
     RadauParams prm;
     double pr;
     Stats& stats;
+    const LearnArgs* learn = nullptr;   // block teams only: learned proposals / step records
+
+    // MLP input features of the calling thread's element (raw; standardised in mlp_infer_team)
+    __device__ __forceinline__ void mlp_features(const V& y, double Hprev, float* x) const {
+        const int l = TM::lane();
+        float f = 0.0f;
+        if (l == 0) f = float(y[0]);
+        else if (l < N) f = float(log10(fmax(y[0], 1e-20)));
+        else if (l == N) f = float(log10(Hprev));
+        else if (l == N + 1) f = float(log10(pr / 101325.0));
+        for (int i = l; i < MLP_D0; i += TS) x[i] = (i == l) ? f : 0.0f;
+    }
+
+    // Append one step record (features at the step start, converged stages, accepted H).
+    __device__ void record_step(const V& y, double Hprev, double H, const V& Z1, const V& Z2, const V& Z3) {
+        int slot = 0;
+        if (TM::lane() == 0) slot = atomicAdd(learn->rec_count, 1);
+        slot = TM::bcast(slot, 0);
+        if (slot >= learn->rec_cap) return;
+        float* r = learn->rec + size_t(slot) * MLP_REC;
+        mlp_features(y, Hprev, r);
+        float* tg = r + MLP_D0;
+        const int l = TM::lane();
+        if (l < N) {
+            const double si = prm.atol + prm.rtol * fabs(y[0]);
+            tg[l] = float(symlog(Z1[0] / si));
+            tg[N + l] = float(symlog(Z2[0] / si));
+            tg[2 * N + l] = float(symlog(Z3[0] / si));
+        }
+        for (int i = 3 * N + l; i < MLP_D4; i += TS) tg[i] = (i == 3 * N) ? float(log10(H)) : 0.0f;
+    }
 
     __device__ __forceinline__ void rhs(double t, const V& y, V& f) {
         mech.template dydt<TS>(t, pr, y, f, st.scratch_rhs());
@@ -364,8 +398,46 @@ struct Radau {
         }
         int Nconsecutive = 0, Nsteps = 0;
         double NewtonRate = pow(2.0, 1.25);
+        // learned mode (block teams): proposals for the stages (ZP*) and the step size
+        int mlp_flags = 0;
+        if constexpr (LEARN) {
+            if (learn) mlp_flags = learn->mlp.flags;
+        }
+        double Hprev = H;   // last accepted step size (the model's h feature)
+        bool have_zp = false;
+        V ZP1, ZP2, ZP3;
         while (t + radau::ROUNDOFF < t_end) {
             if (!Reject) rhs(t, y, F0);
+            if constexpr (LEARN) {
+                if (mlp_flags && !Reject) {
+                    float* xb = reinterpret_cast<float*>(st.scratch_rhs());
+                    mlp_features(y, Hprev, xb);
+                    TM::sync();
+                    const float* o = mlp_infer_team<TS>(learn->mlp, xb, xb + MLP_D0, xb + MLP_D0 + MLP_D4);
+                    const double Hp = exp10(double(o[3 * N]));
+                    if (mlp_flags & MLP_USE_Z) {
+#pragma unroll
+                        for (int s = 0; s < S; ++s) {
+                            const int i = V::idx(s);
+                            const double si = ATOL + RTOL * fabs(y[s]);
+                            ZP1[s] = V::ok(s) ? symexp(double(o[i])) * si : 0.0;
+                            ZP2[s] = V::ok(s) ? symexp(double(o[N + i])) * si : 0.0;
+                            ZP3[s] = V::ok(s) ? symexp(double(o[2 * N + i])) * si : 0.0;
+                        }
+                        have_zp = true;
+                    }
+                    TM::sync();
+                    if ((mlp_flags & MLP_USE_H) && Hp == Hp) {
+                        // never above the controller's step, never below 1/8 of it
+                        const double Hn = fmin(H, fmax(Hp, 0.125 * H));
+                        if (Hn != H) {
+                            H = Hn;
+                            SkipLU = false;
+                        }
+                    }
+                    stats.c[ST_KRYLOV]++;
+                }
+            }
             if (!SkipLU) {
                 if (!SkipJac) {
                     mech.template jacob<TS>(t, pr, y, st.jac(), st.scratch_jac());
@@ -388,7 +460,17 @@ struct Radau {
             stats.c[ST_STEPS]++;
             if (Nsteps >= radau::MAX_NO_STEPS) return EC_max_steps_exceeded;
             if (0.1 * fabs(H) <= fabs(t) * radau::ROUNDOFF) return EC_h_plus_t_equals_h;
-            if (FirstStep) {
+            NewtonRate = pow(fmax(NewtonRate, DBL_EPSILON), 0.8);
+            bool NewtonDone = false;
+            double Fac = 0.5;
+            int NewtonIter = 0;
+            double Theta = 0;
+            for (int attempt = 0; attempt < 2; ++attempt) {
+            const bool use_zp = have_zp && attempt == 0;
+            if (use_zp) {
+#pragma unroll
+                for (int s = 0; s < S; ++s) { Z1[s] = ZP1[s]; Z2[s] = ZP2[s]; Z3[s] = ZP3[s]; }
+            } else if (FirstStep) {
 #pragma unroll
                 for (int s = 0; s < S; ++s) Z1[s] = Z2[s] = Z3[s] = 0.0;
             } else {
@@ -401,12 +483,11 @@ struct Radau {
                     Z3[s] = CONT0[s] + x2 * (CONT1[s] + x3 * CONT2[s]);
                 }
             }
-            bool NewtonDone = false;
+            NewtonDone = false;
             double NewtonIncrementOld = 0;
-            double Fac = 0.5;
-            int NewtonIter = 0;
-            double Theta = 0;
-            NewtonRate = pow(fmax(NewtonRate, DBL_EPSILON), 0.8);
+            Fac = 0.5;
+            NewtonIter = 0;
+            Theta = 0;
             for (; NewtonIter < radau::NEWTON_MAXIT; NewtonIter++) {
                 stats.c[ST_NEWTON]++;
                 // RK_PrepareRHS (radau2a.c:353-383)
@@ -455,8 +536,15 @@ struct Radau {
                 }
                 NewtonDone = (NewtonRate * NewtonIncrement <= radau::NEWTON_TOL);
                 if (NewtonDone) break;
-                if (NewtonIter == radau::NEWTON_MAXIT - 1) return EC_newton_max_iterations_exceeded;
+                if (NewtonIter == radau::NEWTON_MAXIT - 1) {
+                    if (use_zp) break;   // learned guess failed: fall back to the extrapolation
+                    return EC_newton_max_iterations_exceeded;
+                }
             }
+            if (NewtonDone || !use_zp) break;
+            stats.c[ST_ARNOLDI]++;   // fall-back to the extrapolated guess, same H and LU
+            }
+            have_zp = false;
             if (!NewtonDone) {
                 H = Fac * H;
                 Reject = true;
@@ -477,6 +565,10 @@ struct Radau {
                     Fac = fmin(Fac, FacGus);
                     Hnew = Fac * H;
                 }
+                if constexpr (LEARN) {
+                    if (learn && learn->rec) record_step(y, Hprev, H, Z1, Z2, Z3);
+                }
+                Hprev = H;
                 Hacc = H;
                 ErrOld = fmax(1e-2, Err);
                 FirstStep = false;

@@ -140,6 +140,53 @@ int accelerInt_get_codes(int* codes_host, int NUM);
  * (exponential_integrators/rational_approximant.c:23-44, cf.c:41-312); no GPU
  * needed.  Conjugate pairs, positive imaginary part first. */
 int accelerInt_get_poles(double* poles_re, double* poles_im, double* res_re, double* res_im);
+/* ---- Learned step proposals (extension; no counterpart in the reference) ----
+ * A multilayer perceptron 64 -> 128 -> 128 -> 128 -> 176 (GELU) maps the state at
+ * the start of a Radau step -- T, log10 max(Y_k, 1e-20), log10 of the last
+ * accepted step size, log10(P / 1 atm) -- to symlog-scaled initial Newton stage
+ * values and log10 of the step size to use.  Parameters are one FP32 vector
+ * (W0 b0 W1 b1 W2 b2 W3 b3, W_l row-major [out x in]); the solver and the
+ * kernels below compute with BF16-rounded weights and activations and FP32
+ * accumulation.  norm holds in_mu[64] in_sd[64] out_mu[176] out_sd[176].
+ * All pointers are device pointers; M (batch) must be a multiple of 16. */
+#define ACCELERINT_MLP_USE_H 1   /* cap the next step size by the proposal (never below 1/8 of the controller's) */
+#define ACCELERINT_MLP_USE_Z 2   /* start Newton from the proposed stages; on failure retry from the extrapolation */
+int accelerInt_mlp_sizes(int* nparam, int* nnorm, int* d_in, int* d_out);
+/* y[M x 176] = de-standardised network output for raw inputs x[M x 64] */
+int accelerInt_mlp_forward(const float* params_dev, const float* norm_dev, const float* x_dev, int M, float* y_dev,
+                           void* stream);
+/* loss = sum_m sum_j w_j (f(xs_m)_j - ts_mj)^2 / M on standardised xs[M x 64], ts[M x 176]; grad[nparam] */
+int accelerInt_mlp_loss_grad(const float* params_dev, const float* xs_dev, const float* ts_dev, const float* w_dev,
+                             int M, float* grad_dev, float* loss_dev, void* stream);
+/* one Adam update (bias-corrected) of the FP32 parameters */
+int accelerInt_mlp_adam_step(float* params_dev, const float* grad_dev, float* m_dev, float* v_dev, int step,
+                             float lr, float beta1, float beta2, float eps, void* stream);
+/* Install (flags != 0) or remove (flags == 0) the model for the mass-action Radau
+ * kernels; the parameter and norm buffers must stay valid while installed. */
+int accelerInt_set_learned(const float* params_dev, const float* norm_dev, int flags);
+/* Capture one record per accepted Radau step (block teams): raw features [64] then
+ * raw targets [176] -- symlog(Z_c,i / (atol + rtol |y_i|)) for c = 1..3, then
+ * log10 H -- into rec_dev[capacity][240]; *count_dev counts records claimed (it may
+ * exceed capacity; the surplus is dropped).  rec_dev == NULL switches capture off. */
+int accelerInt_set_step_recording(float* rec_dev, int* count_dev, int capacity);
+
+/* ---- Launch mapping and CUDA-graph launches (extensions) ----
+ * accelerInt_set_graph_launch(1): accelerInt_integrate_device records each call's
+ * launch sequence (work-queue reset + kernel) by stream capture into a cached
+ * executable graph (updated in place when only the arguments change) and
+ * launches that graph on the caller's stream.
+ * accelerInt_set_launch_config: resident blocks per SM of the persistent team
+ * kernels (0: occupancy maximum) and the block size of the thread-per-system
+ * kernels (0: unchanged).
+ * accelerInt_autotune: times the candidate mappings on a copy of the first
+ * `sample` systems of y_dev for the given interval (y_dev is not modified) and
+ * keeps the fastest; reports the choice and its time. */
+int accelerInt_set_graph_launch(int enable);
+int accelerInt_set_launch_config(int occupancy_cap, int tps_block);
+int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, const double* y_dev,
+                        const double* var_dev, int sample, int* occupancy_cap_out, int* tps_block_out,
+                        double* best_ms_out);
+
 /* Extension: number of kernels this library has launched in the process. */
 long long accelerInt_kernel_launches(void);
 const char* accelerInt_version(void);
