@@ -620,7 +620,7 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
     if (g.mech_kind == 0 && (g.solver == ACCELERINT_RADAU2A || g.solver == ACCELERINT_RKC)) {
         // thread per system: block size
         int best_b = g.tps_block;
-        for (int b : {64, 128, 256, 512}) {
+        for (int b : {32, 64, 128}) {   // the kernels' launch bound is 128 threads
             g.tps_block = b;
             if ((rc = trial(&ms))) break;
             if (ms < best) { best = ms; best_b = b; }

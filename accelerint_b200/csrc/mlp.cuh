@@ -5,8 +5,8 @@
 //          log10 h (the last accepted step size), log10 (P / 1 atm)
 //   hidden 3 x 128, GELU (erf form)
 //   output (D4 = 176, first 3N + 1 used): symlog(Z_c,i / s_i) for the three
-//          stages c and elements i, s_i = atol + rtol |y_i|, then log10 H of the
-//          step the solver accepted from this state.
+//          stages c and elements i, s_i = atol + rtol |y_i|, then log10 of the
+//          accepted step size over the previous accepted one.
 // Inputs and outputs are standardised with per-feature mean / spread stored with
 // the model.  Weights are BF16 (the solver's copy); accumulation is FP32.
 //

@@ -156,7 +156,8 @@ struct Radau {
         for (int i = l; i < MLP_D0; i += TS) x[i] = (i == l) ? f : 0.0f;
     }
 
-    // Append one step record (features at the step start, converged stages, accepted H).
+    // Append one step record (features at the step start, converged stages,
+    // log10 of the accepted H over the previous accepted H).
     __device__ void record_step(const V& y, double Hprev, double H, const V& Z1, const V& Z2, const V& Z3) {
         int slot = 0;
         if (TM::lane() == 0) slot = atomicAdd(learn->rec_count, 1);
@@ -172,7 +173,7 @@ struct Radau {
             tg[N + l] = float(symlog(Z2[0] / si));
             tg[2 * N + l] = float(symlog(Z3[0] / si));
         }
-        for (int i = 3 * N + l; i < MLP_D4; i += TS) tg[i] = (i == 3 * N) ? float(log10(H)) : 0.0f;
+        for (int i = 3 * N + l; i < MLP_D4; i += TS) tg[i] = (i == 3 * N) ? float(log10(H / Hprev)) : 0.0f;
     }
 
     __device__ __forceinline__ void rhs(double t, const V& y, V& f) {
@@ -211,7 +212,12 @@ struct Radau {
             int* inf = st.infos();
             const int w = TM::warp();
             const bool l0 = (threadIdx.x & 31) == 0;
-            if (TS >= 64) {
+            if (TS == 64) {
+                // both warps on E2, then both on E1 (the complex factorisation is ~4x the real one)
+                const int i2 = tlu<N, cx<LT>>(E2, st.perm2(), st.dinv2());
+                const int i1 = tlu<N, L1>(E1, st.perm1(), st.dinv1());
+                if (l0 && w == 0) { inf[0] = i1; inf[1] = i2; }
+            } else if (TS > 64) {
                 if (w == 0) {
                     const int i1 = wlu_real<N, L1>(E1, st.perm1(), st.dinv1());
                     if (l0) inf[0] = i1;
@@ -414,7 +420,7 @@ struct Radau {
                     mlp_features(y, Hprev, xb);
                     TM::sync();
                     const float* o = mlp_infer_team<TS>(learn->mlp, xb, xb + MLP_D0, xb + MLP_D0 + MLP_D4);
-                    const double Hp = exp10(double(o[3 * N]));
+                    const double Hp = Hprev * exp10(double(o[3 * N]));
                     if (mlp_flags & MLP_USE_Z) {
 #pragma unroll
                         for (int s = 0; s < S; ++s) {
@@ -428,8 +434,9 @@ struct Radau {
                     }
                     TM::sync();
                     if ((mlp_flags & MLP_USE_H) && Hp == Hp) {
-                        // never above the controller's step, never below 1/8 of it
-                        const double Hn = fmin(H, fmax(Hp, 0.125 * H));
+                        // limits growth only: never above the controller's step, never
+                        // below the last accepted one
+                        const double Hn = fmin(H, fmax(Hp, Hprev));
                         if (Hn != H) {
                             H = Hn;
                             SkipLU = false;

@@ -59,6 +59,10 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=0, help="systems in the CPU baseline sample (0: auto)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--learned", type=int, default=0, choices=[0, 1, 2, 3],
+                   help="learned proposals in the tuned form: 1 step size, 2 stages, 3 both (0: off)")
+    p.add_argument("--train-num", type=int, default=4096,
+                   help="systems of the differently seeded batch whose plain Radau steps train the MLP")
     args = p.parse_args()
     if args.plain_steps < 0:
         args.plain_steps = args.steps
@@ -220,7 +224,20 @@ def run_ours(args):
     dev = torch.device("cuda", local if ws > 1 else 0)
     mech, y, var = workload(args.num, args.seed, rank)
     lu = {"fp32": A.LU_FP32, "fp32_all": A.LU_FP32_ALL, "fp64": A.LU_FP64}[args.lu]
+    model, learn_info = None, None
+    if args.learned:
+        # train on plain-Radau step records of a batch drawn with another seed (untimed)
+        from accelerint_b200 import learned as Lm
+        t0 = time.time()
+        yt, vt = M.mixed_stiffness_initial_conditions(mech, args.train_num, args.seed + 104729 + rank)
+        rec = Lm.record_steps(mech, yt, vt, 0.0, DT, DT, capacity=1 << 22, device=dev.index)
+        model = Lm.train(rec, mech.n_state, epochs=30)
+        learn_info = {"flags": args.learned, "train_systems": args.train_num, "records": int(rec.shape[0]),
+                      "holdout_loss": model.history[-1], "train_s": time.time() - t0}
+        del rec
     integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu)
+    if model is not None:
+        model.install(integ, args.learned)
     stream = torch.cuda.Stream(device=dev)
     y0 = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
     vd = torch.from_numpy(np.ascontiguousarray(var)).to(dev)
@@ -323,11 +340,12 @@ def run_ours(args):
                 "data": "synthetic",
                 "config": {"workload": f"mass-action 53 species / 325 reactions, mixed stiffness, {args.num} ICs "
                                        f"per GPU, global steps of dt=1e-6 s from t=0, {args.solver} rtol 1e-6 "
-                                       f"atol 1e-10, LU {args.lu}, persistent work-queue team kernel",
+                                       f"atol 1e-10, LU {args.lu}, persistent work-queue team kernel"
+                                       + (f", learned proposals {args.learned}" if args.learned else ""),
                            "l2": f"L2 flushed (256 MiB write) before every timed step; state y is {mb:.0f} MB",
                            "failed_systems": nfail},
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain}
+                "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain, "learned": learn_info}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist

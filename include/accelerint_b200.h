@@ -144,12 +144,12 @@ int accelerInt_get_poles(double* poles_re, double* poles_im, double* res_re, dou
  * A multilayer perceptron 64 -> 128 -> 128 -> 128 -> 176 (GELU) maps the state at
  * the start of a Radau step -- T, log10 max(Y_k, 1e-20), log10 of the last
  * accepted step size, log10(P / 1 atm) -- to symlog-scaled initial Newton stage
- * values and log10 of the step size to use.  Parameters are one FP32 vector
+ * values and log10 of the next step size over the last accepted one.  Parameters are one FP32 vector
  * (W0 b0 W1 b1 W2 b2 W3 b3, W_l row-major [out x in]); the solver and the
  * kernels below compute with BF16-rounded weights and activations and FP32
  * accumulation.  norm holds in_mu[64] in_sd[64] out_mu[176] out_sd[176].
  * All pointers are device pointers; M (batch) must be a multiple of 16. */
-#define ACCELERINT_MLP_USE_H 1   /* cap the next step size by the proposal (never below 1/8 of the controller's) */
+#define ACCELERINT_MLP_USE_H 1   /* limit step growth to the proposal: min(controller, max(proposal, last accepted)) */
 #define ACCELERINT_MLP_USE_Z 2   /* start Newton from the proposed stages; on failure retry from the extrapolation */
 int accelerInt_mlp_sizes(int* nparam, int* nnorm, int* d_in, int* d_out);
 /* y[M x 176] = de-standardised network output for raw inputs x[M x 64] */
@@ -166,7 +166,7 @@ int accelerInt_mlp_adam_step(float* params_dev, const float* grad_dev, float* m_
 int accelerInt_set_learned(const float* params_dev, const float* norm_dev, int flags);
 /* Capture one record per accepted Radau step (block teams): raw features [64] then
  * raw targets [176] -- symlog(Z_c,i / (atol + rtol |y_i|)) for c = 1..3, then
- * log10 H -- into rec_dev[capacity][240]; *count_dev counts records claimed (it may
+ * log10(H / H_previous) -- into rec_dev[capacity][240]; *count_dev counts records claimed (it may
  * exceed capacity; the surplus is dropped).  rec_dev == NULL switches capture off. */
 int accelerInt_set_step_recording(float* rec_dev, int* count_dev, int capacity);
 
