@@ -410,6 +410,7 @@ void accelerInt_cleanup(void) {
     g.cap_stream = nullptr;
     g.occ_cap = 0;
     g.tps_block = 128;
+    g.graph = false;
     g.learn = LearnArgs{};
     if (g.dev_tb_mem) cudaFree(g.dev_tb_mem);
     if (g.stream) cudaStreamDestroy(g.stream);

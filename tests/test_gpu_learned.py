@@ -7,10 +7,13 @@
 * Training on step records of plain Radau runs lowers the held-out loss.
 * What the trained network gains: on a differently seeded batch of the
   53-species mixed-stiffness workload, Radau with the learned step-size
-  proposals rejects fewer steps (the plain method's rejections are almost all
-  Newton failures after the controller grows the step) and needs fewer LU
-  factorisations, while its results stay as accurate as the plain method's
-  against a tight FP64 oracle (rtol 1e-12).
+  proposals rejects far fewer steps (the plain method's rejections are almost
+  all Newton failures after the controller grows the step), while its results
+  stay as accurate as the plain method's against a tight FP64 oracle (rtol
+  1e-12).  The test prints the step, factorisation and Newton counts of both:
+  the proposals also hold back growth where the plain controller's growth
+  succeeds, so total work is not reduced -- on the bench workload the learned
+  form is slower, and the bench runs it only on request (--learned).
 """
 import numpy as np
 import pytest
@@ -109,8 +112,7 @@ def test_learned_step_size_gain(trained, oracle):
           f"\nlearned: steps {learned[0]} rejected {learned[2]} decomp {learned[4]} newton {learned[5]} "
           f"proposals {learned[8]}")
     assert learned[8] > 0
-    assert learned[2] < plain[2]          # fewer rejected steps
-    assert learned[4] < plain[4]          # fewer factorisations
+    assert learned[2] < 0.5 * plain[2]    # rejected steps at least halved
     # accuracy against the tight oracle on a subsample: no worse than the plain method's
     sub = np.arange(0, 512, 16)
     yt, _, _ = oracle.run("radau2a", mech, y[:, sub], var[sub], 0.0, 1e-6, 1e-6, rtol=1e-12, atol=1e-20)
