@@ -31,7 +31,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_measure_fma_peak", "accelerInt_integrate_device_noalloc", "accelerInt_kernel_launches",
     "accelerInt_mlp_sizes", "accelerInt_mlp_forward", "accelerInt_mlp_loss_grad", "accelerInt_mlp_adam_step",
     "accelerInt_set_learned", "accelerInt_set_step_recording", "accelerInt_set_graph_launch",
-    "accelerInt_set_launch_config", "accelerInt_autotune",
+    "accelerInt_set_launch_config", "accelerInt_autotune", "accelerInt_set_persistent",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -68,6 +68,7 @@ def load_library():
     lib.accelerInt_set_learned.argtypes = [vp, vp, i]
     lib.accelerInt_set_step_recording.argtypes = [vp, vp, i]
     lib.accelerInt_set_graph_launch.argtypes = [i]
+    lib.accelerInt_set_persistent.argtypes = [i]
     lib.accelerInt_set_launch_config.argtypes = [i, i]
     lib.accelerInt_autotune.argtypes = [i, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, i, vp, vp, vp]
     lib.accelerInt_kernel_launches.argtypes = []
@@ -154,6 +155,9 @@ class Integrator:
                                                  var_dev.data_ptr(), int(sample), ctypes.byref(occ),
                                                  ctypes.byref(blk), ctypes.byref(ms)))
         return occ.value, blk.value, ms.value
+
+    def set_persistent(self, enable: bool = True):
+        self._check(self.lib.accelerInt_set_persistent(1 if enable else 0))
 
     def set_graph_launch(self, enable: bool = True):
         self._check(self.lib.accelerInt_set_graph_launch(1 if enable else 0))

@@ -77,6 +77,7 @@ struct State {
     int tps_block = 128;
     int last_occ = 0;             // resident blocks per SM of the last team launch
     bool graph = false;           // device-buffer launches through a captured CUDA graph
+    bool persistent = true;       // team kernels: persistent grid + work queue (else one team per system)
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;
 };
@@ -191,10 +192,16 @@ int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
     int grid = 0;
     int rc = persistent_grid(kern, block, smem, a.num, tpb, &grid);
     if (rc) return rc;
+    if (!g.persistent) {
+        // plain form: one team per system over a full grid (the hardware block
+        // scheduler balances), one Jacobian per system
+        grid = (a.num + tpb - 1) / tpb;
+        a.plain_grid = 1;
+    }
     rc = ensure_jac(size_t(grid) * tpb * N * N);
     if (rc) return rc;
     a.jac = g.jac;
-    CK(cudaMemsetAsync(a.queue, 0, sizeof(int), s));
+    if (g.persistent) CK(cudaMemsetAsync(a.queue, 0, sizeof(int), s));
     kern<<<grid, block, smem, s>>>(a, mech, lay);
     CK(cudaGetLastError());
     g.launches++;
@@ -411,6 +418,7 @@ void accelerInt_cleanup(void) {
     g.occ_cap = 0;
     g.tps_block = 128;
     g.graph = false;
+    g.persistent = true;
     g.learn = LearnArgs{};
     if (g.dev_tb_mem) cudaFree(g.dev_tb_mem);
     if (g.stream) cudaStreamDestroy(g.stream);
@@ -563,6 +571,11 @@ int accelerInt_set_learned(const float* params_dev, const float* norm_dev, int f
     g.learn.mlp.p = params_dev;
     g.learn.mlp.norm = norm_dev;
     g.learn.mlp.flags = flags;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_persistent(int enable) {
+    g.persistent = enable != 0;
     return ACCELERINT_OK;
 }
 

@@ -31,6 +31,7 @@ struct BatchArgs {
     double* jac;            // per-team Jacobian scratch [teams * N * N]
     double atol, rtol;
     LearnArgs learn;        // Radau block teams: learned proposals / step records (zero: off)
+    int plain_grid;         // team kernels: one team per system over a full grid, no work queue
 };
 
 // The reference's global-step loop (generic/solver_main.c:196-209), measured from t_start.
@@ -164,10 +165,15 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
     const int gteam = blockIdx.x * tpb + tib;
     unsigned char* base = smem + size_t(tib) * lay.total;
     const int lane = TM::lane();
-    for (;;) {
+    for (int it = 0;; ++it) {
         int sys = 0;
-        if (lane == 0) sys = atomicAdd(a.queue, 1);
-        sys = TM::bcast(sys, 0);
+        if (a.plain_grid) {
+            if (it > 0) break;
+            sys = gteam;
+        } else {
+            if (lane == 0) sys = atomicAdd(a.queue, 1);
+            sys = TM::bcast(sys, 0);
+        }
         if (sys >= a.num) break;
         Vec<N, TS> y;
 #pragma unroll

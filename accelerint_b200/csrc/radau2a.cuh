@@ -415,7 +415,9 @@ struct Radau {
         while (t + radau::ROUNDOFF < t_end) {
             if (!Reject) rhs(t, y, F0);
             if constexpr (LEARN) {
-                if (mlp_flags && !Reject) {
+                // the step-size proposal can only bind when the controller grows the
+                // step more than 2x; stage proposals are wanted on every step
+                if (mlp_flags && !Reject && ((mlp_flags & MLP_USE_Z) || H > 2.0 * Hprev)) {
                     float* xb = reinterpret_cast<float*>(st.scratch_rhs());
                     mlp_features(y, Hprev, xb);
                     TM::sync();
@@ -434,9 +436,10 @@ struct Radau {
                     }
                     TM::sync();
                     if ((mlp_flags & MLP_USE_H) && Hp == Hp) {
-                        // limits growth only: never above the controller's step, never
-                        // below the last accepted one
-                        const double Hn = fmin(H, fmax(Hp, Hprev));
+                        // limits growth only: never above the controller's step, and
+                        // never below twice the last accepted one, so the proposal cannot
+                        // hold the step size down
+                        const double Hn = fmin(H, fmax(Hp, 2.0 * Hprev));
                         if (Hn != H) {
                             H = Hn;
                             SkipLU = false;

@@ -13,8 +13,14 @@ conditions, then the state is reset), so the transient after t = 0 is always
 inside the timed region.  L2 is flushed (a 256 MiB write) between timed steps,
 outside the per-step event pairs.
 
-Beside the tuned form (LU in FP32, the default) the plain FP64 form is timed on
-the same batch for `--plain-steps` global steps and reported as "plain_fp64".
+The tuned form is the three north-star changes on top of the plain FP64 form:
+E1/E2 factorised and solved in FP32 (--lu), the persistent work-queue kernel
+under a captured CUDA graph with the autotuned mapping, and the learned
+step-size proposals (--learned; the MLP is trained, untimed, on plain Radau
+step records of a batch drawn with another seed).  The plain FP64 form (one
+team per system over a plain grid, FP64 factorisations, no proposals) is timed
+on the same batch for `--plain-steps` global steps and reported as
+"plain_fp64" with the tuned / plain ratio.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--lu fp32|fp64] [--num NUM] [--solver radau2a]
@@ -61,7 +67,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--no-graph", action="store_true")
-    p.add_argument("--learned", type=int, default=0, choices=[0, 1, 2, 3],
+    p.add_argument("--learned", type=int, default=1, choices=[0, 1, 2, 3],
                    help="learned proposals in the tuned form: 1 step size, 2 stages, 3 both (0: off)")
     p.add_argument("--train-num", type=int, default=4096,
                    help="systems of the differently seeded batch whose plain Radau steps train the MLP")
@@ -315,7 +321,10 @@ def run_ours(args):
     # the plain FP64 form on the same batch, for the tuned-vs-plain ratio
     plain = None
     if args.plain_steps > 0 and args.lu != "fp64":
+        # the plain form: FP64 factorisations, one team per system over a plain grid
+        # (no work queue, no graph, no tuning)
         pinteg = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=A.LU_FP64)
+        pinteg.set_persistent(False)
         nw = min(args.num, 4 * 148)
         yw = y0[:, :nw].contiguous()
         pinteg.integrate_device(0.0, DT, DT, yw, vd[:nw].contiguous(), None, None, stream)   # warm-up

@@ -149,7 +149,7 @@ int accelerInt_get_poles(double* poles_re, double* poles_im, double* res_re, dou
  * kernels below compute with BF16-rounded weights and activations and FP32
  * accumulation.  norm holds in_mu[64] in_sd[64] out_mu[176] out_sd[176].
  * All pointers are device pointers; M (batch) must be a multiple of 16. */
-#define ACCELERINT_MLP_USE_H 1   /* limit step growth to the proposal: min(controller, max(proposal, last accepted)) */
+#define ACCELERINT_MLP_USE_H 1   /* limit step growth: min(controller, max(proposal, 2 x last accepted)) */
 #define ACCELERINT_MLP_USE_Z 2   /* start Newton from the proposed stages; on failure retry from the extrapolation */
 int accelerInt_mlp_sizes(int* nparam, int* nnorm, int* d_in, int* d_out);
 /* y[M x 176] = de-standardised network output for raw inputs x[M x 64] */
@@ -182,6 +182,11 @@ int accelerInt_set_step_recording(float* rec_dev, int* count_dev, int capacity);
  * `sample` systems of y_dev for the given interval (y_dev is not modified) and
  * keeps the fastest; reports the choice and its time. */
 int accelerInt_set_graph_launch(int enable);
+/* enable = 1 (default): the team kernels run a persistent grid (resident
+ * blocks x SMs) whose teams pull systems from a device work queue.  enable = 0:
+ * the plain form, one team per system over a grid of NUM teams (one Jacobian
+ * scratch per system). */
+int accelerInt_set_persistent(int enable);
 int accelerInt_set_launch_config(int occupancy_cap, int tps_block);
 int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, const double* y_dev,
                         const double* var_dev, int sample, int* occupancy_cap_out, int* tps_block_out,

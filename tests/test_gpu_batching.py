@@ -51,6 +51,20 @@ def test_graph_launch_matches_direct_launch(kind):
     assert np.array_equal(y_half, y_half_direct)
 
 
+@pytest.mark.parametrize("kind", ["ma14"])
+def test_plain_grid_matches_persistent_queue(kind):
+    mech, y, var, t0, t1, dt = _case(kind)
+    integ = A.Integrator(y.shape[1], mech)
+    try:
+        y_queue, c_queue = _device_run(integ, y, var, t0, t1, dt)
+        integ.set_persistent(False)
+        y_plain, c_plain = _device_run(integ, y, var, t0, t1, dt)
+    finally:
+        integ.close()
+    assert np.array_equal(c_queue, c_plain)
+    assert np.array_equal(y_queue, y_plain)
+
+
 @pytest.mark.parametrize("kind", ["vdp", "ma14"])
 def test_autotuned_mapping_gives_identical_results(kind):
     import torch
