@@ -199,11 +199,30 @@ struct Radau {
         const int lane = TM::lane();
         // block teams store lu_cols(N) columns, the ones past N zero (see wlinalg.cuh)
         constexpr int NC = Team<TS>::block ? lu_cols(N) : N;
-        for (int e = lane; e < N * NC; e += TS) {
-            const int i = e % N, j = e / N;
-            const double mj = j < N ? -J[e] : 0.0;
-            E1[e] = L1(i == j ? mj + g : mj);
-            E2[e] = cx<LT>{LT(i == j ? mj + ar : mj), LT(i == j ? ai : 0.0)};
+        if constexpr (Team<TS>::block && TS >= N) {
+            // thread i assembles row i; the Jacobian loads of 8 columns are in flight together
+            if (lane < N) {
+                const int i = lane;
+#pragma unroll 1
+                for (int j0 = 0; j0 < NC; j0 += 8) {
+                    double v[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) v[c] = (j0 + c < N) ? -J[i + (j0 + c) * N] : 0.0;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const int j = j0 + c;
+                        E1[i + j * N] = L1(i == j ? v[c] + g : v[c]);
+                        E2[i + j * N] = cx<LT>{LT(i == j ? v[c] + ar : v[c]), LT(i == j ? ai : 0.0)};
+                    }
+                }
+            }
+        } else {
+            for (int e = lane; e < N * NC; e += TS) {
+                const int i = e % N, j = e / N;
+                const double mj = j < N ? -J[e] : 0.0;
+                E1[e] = L1(i == j ? mj + g : mj);
+                E2[e] = cx<LT>{LT(i == j ? mj + ar : mj), LT(i == j ? ai : 0.0)};
+            }
         }
         TM::sync();
         stats.c[ST_DECOMP]++;
@@ -213,10 +232,10 @@ struct Radau {
             const int w = TM::warp();
             const bool l0 = (threadIdx.x & 31) == 0;
             if (TS == 64) {
-                // both warps on E2, then both on E1 (the complex factorisation is ~4x the real one)
-                const int i2 = tlu<N, cx<LT>>(E2, st.perm2(), st.dinv2());
-                const int i1 = tlu<N, L1>(E1, st.perm1(), st.dinv1());
-                if (l0 && w == 0) { inf[0] = i1; inf[1] = i2; }
+                // E2 pivots on warp 1 overlapped with E1 on warp 0, E2 updates on both
+                const int2 ii = tlu_pair<N, L1, cx<LT>>(E1, st.perm1(), st.dinv1(), E2, st.perm2(), st.dinv2(), inf);
+                TM::sync();
+                if (l0 && w == 0) { inf[0] = ii.x; inf[1] = ii.y; }
             } else if (TS > 64) {
                 if (w == 0) {
                     const int i1 = wlu_real<N, L1>(E1, st.perm1(), st.dinv1());
@@ -317,8 +336,13 @@ struct Radau {
             TM::sync();
             const double* J = st.jac();
             double jx = 0.0;
-            if (t < N)
-                for (int j = 0; j < N; ++j) jx = fma(J[t + N * j], buf[j], jx);
+            if (t < N) {
+                // four partial sums: the Jacobian loads are issued together
+                double a[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int j = 0; j < N; ++j) a[j & 3] = fma(J[t + N * j], buf[j], a[j & 3]);
+                jx = (a[0] + a[1]) + (a[2] + a[3]);
+            }
             V r;
             r[0] = t < N ? b[0] - ((radau::GAMMA / H) * x[0] - jx) : 0.0;
             TM::sync();

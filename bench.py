@@ -295,6 +295,8 @@ def run_ours(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_max = float(tt.item())
     nfail = int((codes != 0).sum().item())
+    # a non-finite state with code 0 would make a step look cheap: count them
+    nonfinite = int((~torch.isfinite(yd)).any(dim=0).sum().item())
     st = stats.cpu().numpy().astype(np.float64)
     flops = float(flops_per_system(st).sum())
     value = ws * args.num * args.steps / (t_max / 1000.0)
@@ -363,7 +365,7 @@ def run_ours(args):
                                        f"atol 1e-10, LU {args.lu}, persistent work-queue team kernel"
                                        + (f", learned proposals {args.learned}" if args.learned else ""),
                            "l2": f"L2 flushed (256 MiB write) before every timed step; state y is {mb:.0f} MB",
-                           "failed_systems": nfail,
+                           "failed_systems": nfail, "nonfinite_systems": nonfinite,
                            "mapping": mapping, "launch": "persistent kernel, "
                            + ("captured CUDA graph" if not args.no_graph else "direct launch")},
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
