@@ -718,8 +718,16 @@ __device__ __noinline__ void wsolve_cplx(const cx<T>* A, const cx<T>* dinv, cons
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const AT lr = AT(cur[r].re), li = AT(cur[r].im);
-            xr[r] = fma(bi, li, fma(-br, lr, xr[r]));
-            xi[r] = fma(-bi, lr, fma(-br, li, xi[r]));
+            if constexpr (sizeof(AT) == sizeof(float)) {
+                // (xr, xi) -= (br, bi) (lr, li) as two packed FP32x2 FMAs
+                float2 v = __ffma2_rn(make_float2(-br, -br), make_float2(lr, li), make_float2(xr[r], xi[r]));
+                v = __ffma2_rn(make_float2(bi, -bi), make_float2(li, lr), v);
+                xr[r] = v.x;
+                xi[r] = v.y;
+            } else {
+                xr[r] = fma(bi, li, fma(-br, lr, xr[r]));
+                xi[r] = fma(-bi, lr, fma(-br, li, xi[r]));
+            }
             cur[r] = nxt[r];
         }
     }
@@ -746,8 +754,15 @@ __device__ __noinline__ void wsolve_cplx(const cx<T>* A, const cx<T>* dinv, cons
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const AT ur = AT(cur[r].re), ui = AT(cur[r].im);
-            xr[r] = fma(bi, ui, fma(-br, ur, xr[r]));
-            xi[r] = fma(-bi, ur, fma(-br, ui, xi[r]));
+            if constexpr (sizeof(AT) == sizeof(float)) {
+                float2 v = __ffma2_rn(make_float2(-br, -br), make_float2(ur, ui), make_float2(xr[r], xi[r]));
+                v = __ffma2_rn(make_float2(bi, -bi), make_float2(ui, ur), v);
+                xr[r] = v.x;
+                xi[r] = v.y;
+            } else {
+                xr[r] = fma(bi, ui, fma(-br, ur, xr[r]));
+                xi[r] = fma(-bi, ur, fma(-br, ui, xi[r]));
+            }
             cur[r] = nxt[r];
         }
     }

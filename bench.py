@@ -239,7 +239,7 @@ def run_ours(args):
         t0 = time.time()
         yt, vt = M.mixed_stiffness_initial_conditions(mech, args.train_num, args.seed + 104729 + rank)
         rec = Lm.record_steps(mech, yt, vt, 0.0, args.steps * DT, DT, capacity=1 << 22, device=dev.index)
-        model = Lm.train(rec, mech.n_state, epochs=30)
+        model = Lm.train(rec, mech.n_state, epochs=8, batch=4096, lr=2e-3)
         learn_info = {"flags": args.learned, "train_systems": args.train_num, "records": int(rec.shape[0]),
                       "holdout_loss": model.history[-1], "train_s": time.time() - t0}
         del rec
