@@ -260,122 +260,6 @@ __device__ __forceinline__ float2 cfnma2(float2 nlr, float2 lim, float2 u, float
     return __ffma2_rn(lim, us, __ffma2_rn(nlr, u, a));
 }
 
-// The same factorisation (xGETF2 semantics, as wlu_real / wlu_cplx) by the two
-// warps of a 64-thread block team.  Both warps search the pivot of column k
-// and form its multipliers in registers; the trailing update is split by
-// column parity (warp w owns the columns j with j % 2 == w, 28 of the 56
-// stored).  The owner of column k writes its multipliers at the start of step
-// k + 1, after the block barrier that closes step k, so the other warp never
-// reads a column that is being written and one barrier per step suffices.
-template <int N, typename E>
-__device__ __noinline__ int tlu(E* A, int* perm, E* dinv)
-{
-    constexpr int R = (N + 31) / 32;
-    constexpr int CB = 4;
-    constexpr int NC = lu_cols(N);
-    constexpr int MH = NC / 2;
-    static_assert(MH % CB == 0, "column padding");
-    const int lane = threadIdx.x & 31;
-    const int w = (threadIdx.x >> 5) & 1;
-    const E zero = ezero_value<E>();
-    int info = 0;
-    if (w == 0)
-        for (int i = lane; i < N; i += 32) perm[i] = i;
-    __syncwarp();
-    E lprev[R];
-    E pivprev = zero;
-#pragma unroll
-    for (int r = 0; r < R; ++r) lprev[r] = zero;
-#pragma unroll 1
-    for (int k = 0; k < N; ++k) {
-        // deferred multipliers (and pivot) of column k - 1 by its owner
-        if (k > 0 && ((k - 1) & 1) == w) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = lane + 32 * r;
-                if (i > k - 1 && i < N) A[i + (k - 1) * N] = lprev[r];
-            }
-            if (lane == 0) A[(k - 1) + (k - 1) * N] = pivprev;
-            __syncwarp();
-        }
-        // pivot of column k, rows k..N-1 (both warps, same result)
-        double best = -1.0;
-        int bi = 0x7fffffff;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int i = lane + 32 * r;
-            if (i >= k && i < N) {
-                const double a = emag(A[i + k * N]);
-                if (!(a <= best)) { best = a; bi = i; }
-            }
-        }
-        int p = warp_pivot(best, bi);
-        const E piv = A[p + k * N];
-        const bool nz = !ezero(piv);
-        E rc = zero;
-        if (nz) {
-            rc = erecip(piv);
-        } else {
-            if (info == 0) info = k + 1;
-            p = k;   // no interchange without a pivot (xGETF2)
-        }
-        // multipliers of the rows below k after the interchange of rows k and p
-        E l[R];
-        bool act[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int i = lane + 32 * r;
-            act[r] = i > k && i < N;
-            const E a = act[r] ? ((i == p) ? A[k + k * N] : A[i + k * N]) : zero;
-            l[r] = nz ? emul(a, rc) : a;
-            lprev[r] = l[r];
-        }
-        pivprev = piv;
-        if (w == 0 && lane == 0) {
-            dinv[k] = nz ? rc : zero;
-            if (p != k) { const int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
-        }
-        // interchange rows k and p in the owned columns other than k
-        if (p != k) {
-            const int j = 2 * lane + w;
-            if (j < N && j != k) {
-                const E t = A[k + j * N];
-                A[k + j * N] = A[p + j * N];
-                A[p + j * N] = t;
-            }
-            __syncwarp();
-        }
-        // trailing update of the owned columns j > k, CB owned columns at a time
-        const int mfirst = (k + 1 - w + 1) >> 1;          // first owned m with 2m + w > k
-        E* colp = A + lane;
-#pragma unroll 1
-        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
-            E u[CB], a[R][CB];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const int j = 2 * (m0 + c) + w;
-                u[c] = (j > k) ? A[k + j * N] : zero;
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c)
-                    a[r][c] = act[r] ? colp[32 * r + (2 * (m0 + c) + w) * N] : zero;
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c)
-                    if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = efnma(l[r], u[c], a[r][c]);
-        }
-        __syncthreads();
-    }
-    if (((N - 1) & 1) == w) {
-        if (lane == 0) A[(N - 1) + (N - 1) * N] = pivprev;
-    }
-    __syncthreads();
-    return info;
-}
-
 // E1 and E2 together on the two warps of a 64-thread block team, overlapped:
 // in elimination step k warp 1 finds the E2 pivot and writes the E2
 // multipliers of column k while warp 0 performs the whole step k of E1 (the

@@ -299,11 +299,21 @@ def run_ours(args):
     nonfinite = int((~torch.isfinite(yd)).any(dim=0).sum().item())
     st = stats.cpu().numpy().astype(np.float64)
     flops = float(flops_per_system(st).sum())
+    # work of the timed steps: a global step lasts about max(total work / teams, the
+    # slowest system), so run-to-run changes of the slowest system move the number
+    work = {"radau_steps": int(st[:, 0].sum()), "rejected": int(st[:, 2].sum()), "factorisations": int(st[:, 4].sum()),
+            "newton_iterations": int(st[:, 5].sum()), "rhs": int(st[:, 6].sum()),
+            "max_steps_one_system": int(st[:, 0].max()), "flops": flops}
     value = ws * args.num * args.steps / (t_max / 1000.0)
     peak = measure_fp64_peak(torch) if rank == 0 else None
     achieved = flops / (ms / 1000.0) / 1e12
+    # DRAM bytes per launch from one ncu capture of the tuned kernel (1,480 systems, one
+    # global step: 4.72 MB read + written), scaled by the systems of this launch
+    traffic = 4.72e6 / 1480 * args.num if args.lu != "fp64" else None
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None, "traffic": None,
+                "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                "traffic_unit": "bytes per launch (ncu capture scaled by systems)",
+                "algorithmic_bytes": args.num * (2 * mech.n_state + 1) * 8,
                 "note": "algorithmic FP64 flops from device event counters per system "
                         "(decomp, Newton, RHS, error solves, Jacobians) over the kernel time; "
                         "peak = FP64 FMA microbenchmark measured in this run"}
@@ -369,7 +379,8 @@ def run_ours(args):
                            "mapping": mapping, "launch": "persistent kernel, "
                            + ("captured CUDA graph" if not args.no_graph else "direct launch")},
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain, "learned": learn_info}
+                "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain, "learned": learn_info,
+                "work": work}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
