@@ -32,6 +32,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_mlp_sizes", "accelerInt_mlp_forward", "accelerInt_mlp_loss_grad", "accelerInt_mlp_adam_step",
     "accelerInt_set_learned", "accelerInt_set_step_recording", "accelerInt_set_graph_launch",
     "accelerInt_set_launch_config", "accelerInt_autotune", "accelerInt_set_persistent",
+    "accelerInt_set_queue_order", "accelerInt_set_cost_model",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -69,6 +70,8 @@ def load_library():
     lib.accelerInt_set_step_recording.argtypes = [vp, vp, i]
     lib.accelerInt_set_graph_launch.argtypes = [i]
     lib.accelerInt_set_persistent.argtypes = [i]
+    lib.accelerInt_set_queue_order.argtypes = [i]
+    lib.accelerInt_set_cost_model.argtypes = [vp, vp]
     lib.accelerInt_set_launch_config.argtypes = [i, i]
     lib.accelerInt_autotune.argtypes = [i, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, i, vp, vp, vp]
     lib.accelerInt_kernel_launches.argtypes = []
@@ -149,12 +152,15 @@ class Integrator:
 
     def autotune(self, t_start, t_end, stepsize, y_dev, var_dev, sample: int):
         """Pick the launch mapping by timing candidates on a copy of the first `sample` systems.
-        Returns (occupancy cap, thread-per-system block size, best ms)."""
+        Returns (occupancy cap, queue order, thread-per-system block size, best ms)."""
         occ, blk, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         self._check(self.lib.accelerInt_autotune(y_dev.shape[1], t_start, t_end, stepsize, y_dev.data_ptr(),
                                                  var_dev.data_ptr(), int(sample), ctypes.byref(occ),
                                                  ctypes.byref(blk), ctypes.byref(ms)))
-        return occ.value, blk.value, ms.value
+        return occ.value & 0xffff, occ.value >> 16, blk.value, ms.value
+
+    def set_queue_order(self, mode: int):
+        self._check(self.lib.accelerInt_set_queue_order(int(mode)))
 
     def set_persistent(self, enable: bool = True):
         self._check(self.lib.accelerInt_set_persistent(1 if enable else 0))

@@ -17,6 +17,8 @@ int poles_residues(int n, double atol, double* pr, double* pi, double* rr, doubl
 }
 namespace aib_mlp {
 int to_bf16(const float* params, void* w_bf16, cudaStream_t s);
+int predict_cost(const float* params, const float* norm, int num, int n, const double* y, const double* var,
+                 double h, float* x, float* out, float* key, cudaStream_t s);
 }
 
 namespace {
@@ -78,6 +80,16 @@ struct State {
     int last_occ = 0;             // resident blocks per SM of the last team launch
     bool graph = false;           // device-buffer launches through a captured CUDA graph
     bool persistent = true;       // team kernels: persistent grid + work queue (else one team per system)
+    int order_mode = 0;           // work-queue order: 0 index, 1 by y_0 (descending), 2 by last call's steps
+    int order_cap = 0;            // systems the order buffers hold
+    int* order_buf = nullptr;     // [order_cap] queue slot -> system
+    int* cost_buf = nullptr;      // [order_cap] steps of the last call per system (-1: unknown)
+    float* key_buf = nullptr;     // [order_cap] sort keys
+    int* hist_buf = nullptr;      // [ORDER_BUCKETS] histogram / offsets, then 2 floats (key min, max)
+    const float* cost_params = nullptr;   // learned cost model (order_mode 3)
+    const float* cost_norm = nullptr;
+    float* cost_x = nullptr;      // [round16(order_cap) x 64] features
+    float* cost_out = nullptr;    // [round16(order_cap) x 176] outputs
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;
 };
@@ -183,6 +195,56 @@ template <class K> int persistent_grid(K kernel, int block, size_t smem, int num
     return ACCELERINT_OK;
 }
 
+// Longest-first queue order for this launch (order_mode 1 or 2), on stream s.
+int build_order(BatchArgs& a, cudaStream_t s) {
+    if (a.num > g.order_cap) {
+        if (g.order_buf) cudaFree(g.order_buf);
+        if (g.cost_buf) cudaFree(g.cost_buf);
+        if (g.key_buf) cudaFree(g.key_buf);
+        if (g.hist_buf) cudaFree(g.hist_buf);
+        g.order_buf = g.cost_buf = g.hist_buf = nullptr;
+        g.key_buf = nullptr;
+        g.order_cap = 0;
+        CK(cudaMalloc(&g.order_buf, size_t(a.num) * sizeof(int)));
+        CK(cudaMalloc(&g.cost_buf, size_t(a.num) * sizeof(int)));
+        CK(cudaMalloc(&g.key_buf, size_t(a.num) * sizeof(float)));
+        CK(cudaMalloc(&g.hist_buf, (ORDER_BUCKETS + 2) * sizeof(int)));
+        if (g.cost_x) cudaFree(g.cost_x);
+        if (g.cost_out) cudaFree(g.cost_out);
+        g.cost_x = g.cost_out = nullptr;
+        const size_t M = size_t(a.num + 15) / 16 * 16;
+        CK(cudaMalloc(&g.cost_x, M * MLP_D0 * sizeof(float)));
+        CK(cudaMalloc(&g.cost_out, M * MLP_D4 * sizeof(float)));
+        CK(cudaMemsetAsync(g.cost_buf, 0xff, size_t(a.num) * sizeof(int), s));   // -1: unknown
+        g.order_cap = a.num;
+    }
+    float* kmin = reinterpret_cast<float*>(g.hist_buf + ORDER_BUCKETS);
+    float* kmax = kmin + 1;
+    CK(cudaMemsetAsync(g.hist_buf, 0, ORDER_BUCKETS * sizeof(int), s));
+    CK(cudaMemsetAsync(kmin, 0x7f, sizeof(float), s));   // 0x7f7f7f7f: a large positive float
+    CK(cudaMemsetAsync(kmax, 0, sizeof(float), s));
+    const int b = 256, nb = (a.num + b - 1) / b;
+    const int* cost = g.order_mode == 2 ? g.cost_buf : nullptr;
+    const float* ext = nullptr;
+    if (g.order_mode == 3 && g.cost_params) {
+        // learned cost of every system from its state (batched MLP on the tensor cores)
+        const int k = aib_mlp::predict_cost(g.cost_params, g.cost_norm, a.num, state_n(), a.y, a.var,
+                                            a.t_end - a.t_start, g.cost_x, g.cost_out, g.key_buf, s);
+        if (k < 0) return ACCELERINT_ERR_CUDA;
+        g.launches += k;
+        ext = g.key_buf;
+    }
+    order_keys_kernel<<<nb, b, 0, s>>>(a.num, a.y, cost, ext, g.key_buf, kmin, kmax);
+    order_hist_kernel<<<nb, b, 0, s>>>(a.num, g.key_buf, kmin, kmax, g.hist_buf);
+    order_scan_kernel<<<1, ORDER_BUCKETS, 0, s>>>(g.hist_buf);
+    order_scatter_kernel<<<nb, b, 0, s>>>(a.num, g.key_buf, kmin, kmax, g.hist_buf, g.order_buf);
+    CK(cudaGetLastError());
+    g.launches += 4;
+    a.order = g.order_buf;
+    a.cost = g.order_mode == 2 ? g.cost_buf : nullptr;
+    return ACCELERINT_OK;
+}
+
 template <int SK, class Mech, int TS, typename LT, typename L1 = LT, bool LEARN = false>
 int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
     constexpr int N = Mech::N;
@@ -201,6 +263,10 @@ int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
     rc = ensure_jac(size_t(grid) * tpb * N * N);
     if (rc) return rc;
     a.jac = g.jac;
+    if (g.persistent && g.order_mode != 0 && a.num > 0) {
+        rc = build_order(a, s);
+        if (rc) return rc;
+    }
     if (g.persistent) CK(cudaMemsetAsync(a.queue, 0, sizeof(int), s));
     kern<<<grid, block, smem, s>>>(a, mech, lay);
     CK(cudaGetLastError());
@@ -419,6 +485,18 @@ void accelerInt_cleanup(void) {
     g.tps_block = 128;
     g.graph = false;
     g.persistent = true;
+    g.order_mode = 0;
+    if (g.order_buf) cudaFree(g.order_buf);
+    if (g.cost_buf) cudaFree(g.cost_buf);
+    if (g.key_buf) cudaFree(g.key_buf);
+    if (g.hist_buf) cudaFree(g.hist_buf);
+    g.order_buf = g.cost_buf = g.hist_buf = nullptr;
+    g.key_buf = nullptr;
+    g.order_cap = 0;
+    if (g.cost_x) cudaFree(g.cost_x);
+    if (g.cost_out) cudaFree(g.cost_out);
+    g.cost_x = g.cost_out = nullptr;
+    g.cost_params = g.cost_norm = nullptr;
     g.learn = LearnArgs{};
     if (g.dev_tb_mem) cudaFree(g.dev_tb_mem);
     if (g.stream) cudaStreamDestroy(g.stream);
@@ -579,6 +657,26 @@ int accelerInt_set_persistent(int enable) {
     return ACCELERINT_OK;
 }
 
+int accelerInt_set_cost_model(const float* params_dev, const float* norm_dev) {
+    if ((params_dev == nullptr) != (norm_dev == nullptr)) return ACCELERINT_ERR_ARGUMENT;
+    g.cost_params = params_dev;
+    g.cost_norm = norm_dev;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_queue_order(int mode) {
+    if (mode < 0 || mode > 3) return ACCELERINT_ERR_ARGUMENT;
+    if (mode == 3 && !g.cost_params) return ACCELERINT_ERR_STATE;
+    g.order_mode = mode;
+    // the step-count history starts over: the next call orders by y_0 (after any
+    // launch still writing step counts has finished)
+    if (g.cost_buf) {
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemset(g.cost_buf, 0xff, size_t(g.order_cap) * sizeof(int)));
+    }
+    return ACCELERINT_OK;
+}
+
 int accelerInt_set_graph_launch(int enable) {
     g.graph = enable != 0;
     return ACCELERINT_OK;
@@ -655,12 +753,24 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
             }
         }
         g.occ_cap = best_c;
+        // queue order: index order vs longest (hottest) first, at the chosen occupancy
+        if (!rc && g.persistent) {
+            const int keep = g.order_mode;
+            int best_o = keep;
+            for (int o : {0, 1}) {
+                if (o == keep) continue;
+                g.order_mode = o;
+                if ((rc = trial(&ms))) break;
+                if (ms < best) { best = ms; best_o = o; }
+            }
+            g.order_mode = best_o;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(ys);
     if (rc) return rc;
-    if (occupancy_cap_out) *occupancy_cap_out = g.occ_cap;
+    if (occupancy_cap_out) *occupancy_cap_out = g.occ_cap | (g.order_mode << 16);
     if (tps_block_out) *tps_block_out = g.tps_block;
     if (best_ms_out) *best_ms_out = best;
     return ACCELERINT_OK;

@@ -32,6 +32,8 @@ struct BatchArgs {
     double atol, rtol;
     LearnArgs learn;        // Radau block teams: learned proposals / step records (zero: off)
     int plain_grid;         // team kernels: one team per system over a full grid, no work queue
+    const int* order;       // queue order (system index of each queue slot), or null: index order
+    int* cost;              // per-system steps of this call (written), or null
 };
 
 // The reference's global-step loop (generic/solver_main.c:196-209), measured from t_start.
@@ -171,7 +173,10 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             if (it > 0) break;
             sys = gteam;
         } else {
-            if (lane == 0) sys = atomicAdd(a.queue, 1);
+            if (lane == 0) {
+                sys = atomicAdd(a.queue, 1);
+                if (a.order && sys < a.num) sys = a.order[sys];
+            }
             sys = TM::bcast(sys, 0);
         }
         if (sys >= a.num) break;
@@ -234,8 +239,73 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             if (Vec<N, TS>::ok(s)) a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] = y[s];
         if (a.codes && lane == 0) a.codes[sys] = code;
         store_stats<N, TS>(a, sys, st);
+        if (a.cost && lane == 0) a.cost[sys] = st.c[ST_STEPS];
         TM::sync();
     }
+}
+
+// ------------------------------------------------------------- queue order
+// Longest-first order of the work queue by a per-system cost key: keys are
+// mapped to ORDER_BUCKETS buckets between their minimum and maximum (largest
+// key first) and systems are scattered by bucket (counting sort; the order
+// inside a bucket is arbitrary).
+constexpr int ORDER_BUCKETS = 1024;
+
+// key[i]: the previous call's step count when it is known (>= 0), else y_0 (the
+// temperature of the mass-action state).
+// (ext: keys given per system, e.g. a learned cost prediction, used as they are.)
+__global__ void order_keys_kernel(int num, const double* y, const int* cost, const float* ext, float* key,
+                                  float* kmin, float* kmax) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float k = 0.f;
+    if (i < num) {
+        k = ext ? ext[i] : ((cost && cost[i] >= 0) ? float(cost[i]) : float(y[i]));
+        if (!(k == k)) k = 0.f;
+        key[i] = k;
+    }
+    float lo = i < num ? k : 3.0e38f, hi = i < num ? k : -3.0e38f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        // float min / max through the ordered integer images of non-negative keys
+        atomicMin(reinterpret_cast<int*>(kmin), __float_as_int(fmaxf(lo, 0.f)));
+        atomicMax(reinterpret_cast<int*>(kmax), __float_as_int(fmaxf(hi, 0.f)));
+    }
+}
+
+__device__ __forceinline__ int order_bucket(float k, float lo, float hi) {
+    const float span = hi - lo;
+    int b = span > 0.f ? int((hi - fmaxf(k, 0.f)) / span * float(ORDER_BUCKETS - 1)) : 0;
+    return min(max(b, 0), ORDER_BUCKETS - 1);
+}
+
+__global__ void order_hist_kernel(int num, const float* key, const float* kmin, const float* kmax, int* hist) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < num) atomicAdd(hist + order_bucket(key[i], *kmin, *kmax), 1);
+}
+
+// exclusive prefix sum of the histogram, one block of ORDER_BUCKETS threads
+__global__ void order_scan_kernel(int* hist) {
+    __shared__ int s[ORDER_BUCKETS];
+    const int t = threadIdx.x;
+    s[t] = hist[t];
+    __syncthreads();
+    for (int o = 1; o < ORDER_BUCKETS; o <<= 1) {
+        const int v = t >= o ? s[t - o] : 0;
+        __syncthreads();
+        s[t] += v;
+        __syncthreads();
+    }
+    hist[t] = t > 0 ? s[t - 1] : 0;
+}
+
+__global__ void order_scatter_kernel(int num, const float* key, const float* kmin, const float* kmax, int* next,
+                                     int* order) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < num) order[atomicAdd(next + order_bucket(key[i], *kmin, *kmax), 1)] = i;
 }
 
 }  // namespace aib

@@ -214,6 +214,29 @@ void forward(const float* params, const float* xs, int M, cudaStream_t s) {
     }
 }
 
+// MLP features of whole states (the layout the solver's records use): x[m] = (T,
+// log10 max(Y_k, 1e-20), log10 h, log10(P / 1 atm), 0...) for system m of
+// y[N * num] (column-major); rows num..M-1 zero.
+__global__ void state_features_kernel(int num, int M, int n, const double* y, const double* var, double h,
+                                      float* x) {
+    const long e = blockIdx.x * long(blockDim.x) + threadIdx.x;
+    if (e >= long(M) * MLP_D0) return;
+    const int m = int(e / MLP_D0), j = int(e % MLP_D0);
+    float v = 0.f;
+    if (m < num) {
+        if (j == 0) v = float(y[m]);
+        else if (j < n) v = float(log10(fmax(y[size_t(j) * num + m], 1e-20)));
+        else if (j == n) v = float(log10(h));
+        else if (j == n + 1) v = float(log10(var[m] / 101325.0));
+    }
+    x[e] = v;
+}
+
+__global__ void column0_kernel(int num, const float* y, float* key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < num) key[i] = y[size_t(i) * MLP_D4];
+}
+
 }  // namespace
 
 namespace aib_mlp {
@@ -221,6 +244,23 @@ namespace aib_mlp {
 int to_bf16(const float* params, void* w_bf16, cudaStream_t s) {
     to_bf16_kernel<<<nblk(MLP_NWEIGHT), 256, 0, s>>>(params, static_cast<__nv_bfloat16*>(w_bf16));
     return cudaGetLastError() == cudaSuccess ? 0 : ACCELERINT_ERR_CUDA;
+}
+
+// Predicted cost (output 0 of the model) of every system of y, into key[num]
+// (a float per system); x and out: scratch of M x 64 and M x 176 floats,
+// M = num rounded up to 16.  Returns the number of kernels launched, < 0 on error.
+int predict_cost(const float* params, const float* norm, int num, int n, const double* y, const double* var,
+                 double h, float* x, float* out, float* key, cudaStream_t s) {
+    const int M = (num + 15) / 16 * 16;
+    if (ensure_work(M)) return -1;
+    state_features_kernel<<<nblk(long(M) * MLP_D0), 256, 0, s>>>(num, M, n, y, var, h, x);
+    standardize_kernel<<<nblk(long(M) * MLP_D0), 256, 0, s>>>(M, MLP_D0, x, norm, norm + MLP_D0, g_work.x);
+    forward(params, g_work.x, M, s);
+    cudaMemcpyAsync(out, g_work.A[MLP_LAYERS - 1], size_t(M) * MLP_D4 * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    destandardize_kernel<<<nblk(long(M) * MLP_D4), 256, 0, s>>>(M, MLP_D4, out, norm + 2 * MLP_D0,
+                                                                norm + 2 * MLP_D0 + MLP_D4);
+    column0_kernel<<<nblk(num), 256, 0, s>>>(num, out, key);
+    return cudaGetLastError() == cudaSuccess ? 5 + 2 * MLP_LAYERS : -1;
 }
 }  // namespace aib_mlp
 

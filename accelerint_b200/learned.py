@@ -89,6 +89,13 @@ class Model:
     norm: object            # CUDA float32 [2*64 + 2*176]
     history: list
 
+    def install_cost(self, integ: Integrator):
+        """Install as the work queue's cost model and switch to learned-cost order."""
+        rc = integ.lib.accelerInt_set_cost_model(_p(self.params), _p(self.norm))
+        rc = rc or integ.lib.accelerInt_set_queue_order(3)
+        if rc != 0:
+            raise RuntimeError(f"installing the cost model failed: {rc}")
+
     def install(self, integ: Integrator, flags: int = MLP_USE_H):
         rc = integ.lib.accelerInt_set_learned(_p(self.params), _p(self.norm), flags)
         if rc != 0:
@@ -137,7 +144,7 @@ def loss_weights(n_state: int, device, h_weight: float = 16.0):
 
 
 def train(rec, n_state: int, epochs: int = 20, batch: int = 1024, lr: float = 1e-3, seed: int = 0,
-          h_weight: float = 16.0, holdout: float = 0.1) -> Model:
+          h_weight: float = 16.0, holdout: float = 0.1, weights=None) -> Model:
     """Adam on the weighted squared error of the standardised targets, with the
     library's forward / backward kernels.  Returns the model with the held-out
     loss after every epoch."""
@@ -159,7 +166,7 @@ def train(rec, n_state: int, epochs: int = 20, batch: int = 1024, lr: float = 1e
 
     xs, ts = standardise(tr)
     xh, th = standardise(hold)
-    w = loss_weights(n_state, dev, h_weight)
+    w = loss_weights(n_state, dev, h_weight) if weights is None else weights.to(dev)
     params = torch.from_numpy(init_params(seed)).to(dev)
     grad = torch.zeros_like(params)
     m1 = torch.zeros_like(params)
@@ -183,3 +190,51 @@ def train(rec, n_state: int, epochs: int = 20, batch: int = 1024, lr: float = 1e
         assert rc == 0
         history.append(float(loss.item()))
     return Model(n_state, params, norm, history)
+
+
+# ---------------------------------------------------------------- cost model
+def state_features(y, var, h):
+    """The model's input features of whole states (as the device kernel builds them):
+    [num, 64] float32 = (T, log10 max(Y_k, 1e-20), log10 h, log10(P / 1 atm), 0...)."""
+    n, num = y.shape
+    x = np.zeros((num, D_IN), dtype=np.float32)
+    x[:, 0] = y[0]
+    x[:, 1:n] = np.log10(np.maximum(y[1:], 1e-20)).T
+    x[:, n] = np.log10(h)
+    x[:, n + 1] = np.log10(var / 101325.0)
+    return x
+
+
+def cost_records(mech, y, var, t0, t1, dt, device: int = 0, lu: int = LU_FP64):
+    """One record per system and global step: the state's features at the step start
+    and, as output 0, log10(1 + Radau steps the plain solver took in that step)."""
+    import torch
+    num = y.shape[1]
+    integ = Integrator(num, mech, device=device, lu=lu)
+    dev = f"cuda:{device}"
+    recs = []
+    try:
+        yd = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
+        vd = torch.from_numpy(np.ascontiguousarray(var)).to(dev)
+        t = t0
+        while t + 1e-300 < t1 - 1e-12 * abs(t1):
+            tn = min(t1, t + dt)
+            st = torch.zeros((num, 10), dtype=torch.int32, device=dev)
+            x = state_features(yd.cpu().numpy(), var, tn - t)
+            integ.integrate_device(t, tn, tn - t, yd, vd, None, st)
+            torch.cuda.synchronize()
+            r = np.zeros((num, REC), dtype=np.float32)
+            r[:, :D_IN] = x
+            r[:, D_IN] = np.log10(1.0 + st[:, 0].cpu().numpy())
+            recs.append(r)
+            t = tn
+    finally:
+        integ.close()
+    return torch.from_numpy(np.concatenate(recs)).to(dev)
+
+
+def train_cost(rec, n_state: int, epochs: int = 60, seed: int = 0) -> Model:
+    import torch
+    w = torch.zeros(D_OUT, dtype=torch.float32)
+    w[0] = 1.0
+    return train(rec, n_state, epochs=epochs, batch=256, lr=2e-3, seed=seed, weights=w)

@@ -15,9 +15,10 @@ outside the per-step event pairs.
 
 The tuned form is the three north-star changes on top of the plain FP64 form:
 E1/E2 factorised and solved in FP32 (--lu), the persistent work-queue kernel
-under a captured CUDA graph with the autotuned mapping, and the learned
-step-size proposals (--learned; the MLP is trained, untimed, on plain Radau
-step records of a batch drawn with another seed).  The plain FP64 form (one
+under a captured CUDA graph with the autotuned mapping and a longest-first
+queue order from a learned per-system cost model (--queue-order 3), and the
+learned step-size proposals (--learned).  Both networks are trained, untimed,
+by the library's kernels on plain Radau runs of batches drawn with other seeds.  The plain FP64 form (one
 team per system over a plain grid, FP64 factorisations, no proposals) is timed
 on the same batch for `--plain-steps` global steps and reported as
 "plain_fp64" with the tuned / plain ratio.
@@ -66,6 +67,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--queue-order", type=int, default=3, choices=[-1, 0, 1, 2, 3],
+                   help="work-queue order (-1: the autotuner's choice; 0 index, 1 hottest first, 2 most steps "
+                        "in the previous call first, its history restarted before the timed region; 3 largest "
+                        "learned cost first)")
     p.add_argument("--no-graph", action="store_true")
     p.add_argument("--learned", type=int, default=1, choices=[0, 1, 2, 3],
                    help="learned proposals in the tuned form: 1 step size, 2 stages, 3 both (0: off)")
@@ -243,9 +248,20 @@ def run_ours(args):
         learn_info = {"flags": args.learned, "train_systems": args.train_num, "records": int(rec.shape[0]),
                       "holdout_loss": model.history[-1], "train_s": time.time() - t0}
         del rec
+    cost_model = None
+    if args.queue_order == 3:
+        from accelerint_b200 import learned as Lm
+        t0 = time.time()
+        yt, vt = M.mixed_stiffness_initial_conditions(mech, 4 * args.train_num, args.seed + 130363 + rank)
+        crec = Lm.cost_records(mech, yt, vt, 0.0, args.steps * DT, DT, device=dev.index, lu=lu)
+        cost_model = Lm.train_cost(crec, mech.n_state)
+        learn_info = dict(learn_info or {}, cost_records=int(crec.shape[0]), cost_holdout_loss=cost_model.history[-1],
+                          cost_train_s=time.time() - t0)
     integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu)
     if model is not None:
         model.install(integ, args.learned)
+    if cost_model is not None:
+        cost_model.install_cost(integ)
     stream = torch.cuda.Stream(device=dev)
     y0 = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
     vd = torch.from_numpy(np.ascontiguousarray(var)).to(dev)
@@ -264,8 +280,13 @@ def run_ours(args):
     mapping = None
     if not args.no_autotune:
         sample = min(args.num, 8 * 740)
-        occ, blk, tms = integ.autotune(0.0, DT / 4, DT / 4, y0, vd, sample)
-        mapping = {"occupancy_cap": occ, "tps_block": blk, "sample_systems": sample, "best_ms": tms}
+        occ, order, blk, tms = integ.autotune(0.0, DT / 4, DT / 4, y0, vd, sample)
+        mapping = {"occupancy_cap": occ, "queue_order": order, "tps_block": blk, "sample_systems": sample,
+                   "best_ms": tms}
+    if args.queue_order >= 0:
+        integ.set_queue_order(args.queue_order)
+        if mapping is not None:
+            mapping["queue_order"] = args.queue_order
     if not args.no_graph:
         integ.set_graph_launch(True)
     # warm-up: W global steps from the initial conditions, then reset
@@ -273,6 +294,10 @@ def run_ours(args):
         for k in range(args.warmup):
             integ.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, codes, None, stream)
         yd.copy_(y0)
+    if args.queue_order >= 0:
+        # a fresh history: the first timed step knows nothing of the warm-up's step counts
+        torch.cuda.synchronize(dev)
+        integ.set_queue_order(args.queue_order)
     barrier()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]

@@ -178,15 +178,28 @@ int accelerInt_set_step_recording(float* rec_dev, int* count_dev, int capacity);
  * accelerInt_set_launch_config: resident blocks per SM of the persistent team
  * kernels (0: occupancy maximum) and the block size of the thread-per-system
  * kernels (0: unchanged).
- * accelerInt_autotune: times the candidate mappings on a copy of the first
- * `sample` systems of y_dev for the given interval (y_dev is not modified) and
- * keeps the fastest; reports the choice and its time. */
+ * accelerInt_set_queue_order: order in which the persistent teams take systems:
+ * 0 index order; 1 largest y_0 first (the temperature of a mass-action state:
+ * hot systems are the stiff ones); 2 most Radau steps in the previous call first
+ * (mode 1 on the first call); 3 largest learned cost first: a model installed
+ * with accelerInt_set_cost_model (the MLP layout above, output 0 = predicted
+ * log10(1 + Radau steps) of the call from the state's features with h = t_end -
+ * t_start) is evaluated for every system on the tensor cores before the launch.
+ * Longest-first order shortens the tail of a launch, whose end waits for the
+ * slowest system.  Every call of this setter starts the step-count history afresh.
+ * accelerInt_autotune: times the candidate mappings (resident blocks per SM,
+ * then queue order 0 / 1; or the thread-per-system block size) on a copy of the
+ * first `sample` systems of y_dev for the given interval (y_dev is not modified)
+ * and keeps the fastest; reports the choice (occupancy_cap_out: cap | order << 16)
+ * and its time. */
 int accelerInt_set_graph_launch(int enable);
 /* enable = 1 (default): the team kernels run a persistent grid (resident
  * blocks x SMs) whose teams pull systems from a device work queue.  enable = 0:
  * the plain form, one team per system over a grid of NUM teams (one Jacobian
  * scratch per system). */
 int accelerInt_set_persistent(int enable);
+int accelerInt_set_queue_order(int mode);
+int accelerInt_set_cost_model(const float* params_dev, const float* norm_dev);
 int accelerInt_set_launch_config(int occupancy_cap, int tps_block);
 int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, const double* y_dev,
                         const double* var_dev, int sample, int* occupancy_cap_out, int* tps_block_out,

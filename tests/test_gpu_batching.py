@@ -65,6 +65,44 @@ def test_plain_grid_matches_persistent_queue(kind):
     assert np.array_equal(y_queue, y_plain)
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+def test_queue_order_gives_identical_results(mode):
+    """Longest-first queue orders (by temperature, then by the last call's step
+    counts) change which team takes which system, not any result."""
+    mech, y, var, t0, t1, dt = _case("ma14")
+    integ = A.Integrator(y.shape[1], mech)
+    try:
+        y_index, _ = _device_run(integ, y, var, t0, t1, dt)
+        integ.set_queue_order(mode)
+        y_first, _ = _device_run(integ, y, var, t0, t1, dt)
+        y_second, _ = _device_run(integ, y, var, t0, t1, dt)    # mode 2: ordered by the first call's steps
+    finally:
+        integ.close()
+    assert np.array_equal(y_index, y_first)
+    assert np.array_equal(y_index, y_second)
+
+
+def test_learned_cost_order_gives_identical_results():
+    """Queue order 3 evaluates a cost model for every system before the launch
+    (an untrained model here: the order is arbitrary, the results must not move)."""
+    import torch
+    from accelerint_b200 import learned as L
+    mech, y, var, t0, t1, dt = _case("ma14")
+    norm = torch.cat([torch.zeros(L.D_IN), torch.ones(L.D_IN), torch.zeros(L.D_OUT), torch.ones(L.D_OUT)]).cuda()
+    model = L.Model(mech.n_state, torch.from_numpy(L.init_params(3)).cuda(), norm, [])
+    integ = A.Integrator(y.shape[1], mech)
+    try:
+        y_index, _ = _device_run(integ, y, var, t0, t1, dt)
+        model.install_cost(integ)
+        y_cost, _ = _device_run(integ, y, var, t0, t1, dt)
+        integ.set_graph_launch(True)
+        y_graph, _ = _device_run(integ, y, var, t0, t1, dt)
+    finally:
+        integ.close()
+    assert np.array_equal(y_index, y_cost)
+    assert np.array_equal(y_index, y_graph)
+
+
 @pytest.mark.parametrize("kind", ["vdp", "ma14"])
 def test_autotuned_mapping_gives_identical_results(kind):
     import torch
@@ -74,10 +112,10 @@ def test_autotuned_mapping_gives_identical_results(kind):
         y_before, _ = _device_run(integ, y, var, t0, t1, dt)
         yd = torch.from_numpy(y).cuda()
         vd = torch.from_numpy(var).cuda()
-        occ, blk, ms = integ.autotune(t0, t1, dt, yd, vd, sample=y.shape[1] // 2)
+        occ, order, blk, ms = integ.autotune(t0, t1, dt, yd, vd, sample=y.shape[1] // 2)
         torch.cuda.synchronize()
         assert np.array_equal(yd.cpu().numpy(), y)          # the sample ran on a copy
-        assert ms > 0 and occ >= 0 and blk in (32, 64, 128)
+        assert ms > 0 and occ >= 0 and order in (0, 1) and blk in (32, 64, 128)
         y_after, _ = _device_run(integ, y, var, t0, t1, dt)
     finally:
         integ.close()
