@@ -245,7 +245,7 @@ int build_order(BatchArgs& a, cudaStream_t s) {
     return ACCELERINT_OK;
 }
 
-template <int SK, class Mech, int TS, typename LT, typename L1 = LT, bool LEARN = false>
+template <int SK, class Mech, int TS, typename LT, typename L1 = LT, int LEARN = 0>
 int launch_team(BatchArgs a, const Mech& mech, TeamLayout lay, cudaStream_t s) {
     constexpr int N = Mech::N;
     const int block = TS >= 32 ? TS : 32, tpb = block / TS;
@@ -295,19 +295,23 @@ int launch_mass_action(BatchArgs a, cudaStream_t s) {
     const int R = g.mt.R;
     constexpr int N = M::N;
     if (g.solver == ACCELERINT_RADAU2A) {
-        const bool learn = a.learn.rec != nullptr || a.learn.mlp.flags != 0;
+        // learned level: 2 with stage proposals, 1 with step-size proposals or records only
+        const int learn = (a.learn.mlp.flags & MLP_USE_Z) ? 2 : (a.learn.rec != nullptr || a.learn.mlp.flags) ? 1 : 0;
         if (g.lu == ACCELERINT_LU_FP32) {
             TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 8);
-            if (learn) return launch_team<SK_RADAU, M, TS, float, double, true>(a, mech, lay, s);
+            if (learn == 2) return launch_team<SK_RADAU, M, TS, float, double, 2>(a, mech, lay, s);
+            if (learn == 1) return launch_team<SK_RADAU, M, TS, float, double, 1>(a, mech, lay, s);
             return launch_team<SK_RADAU, M, TS, float, double>(a, mech, lay, s);
         }
         if (g.lu == ACCELERINT_LU_FP32_ALL) {
             TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 4);
-            if (learn) return launch_team<SK_RADAU, M, TS, float, float, true>(a, mech, lay, s);
+            if (learn == 2) return launch_team<SK_RADAU, M, TS, float, float, 2>(a, mech, lay, s);
+            if (learn == 1) return launch_team<SK_RADAU, M, TS, float, float, 1>(a, mech, lay, s);
             return launch_team<SK_RADAU, M, TS, float, float>(a, mech, lay, s);
         }
         TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
-        if (learn) return launch_team<SK_RADAU, M, TS, double, double, true>(a, mech, lay, s);
+        if (learn == 2) return launch_team<SK_RADAU, M, TS, double, double, 2>(a, mech, lay, s);
+        if (learn == 1) return launch_team<SK_RADAU, M, TS, double, double, 1>(a, mech, lay, s);
         return launch_team<SK_RADAU, M, TS, double>(a, mech, lay, s);
     }
     if (g.solver == ACCELERINT_RKC) {

@@ -155,7 +155,7 @@ struct TeamLayout {
     }
 };
 
-template <int SK, class Mech, int TS, typename LT, typename L1 = LT, bool LEARN = false>
+template <int SK, class Mech, int TS, typename LT, typename L1 = LT, int LEARN = 0>
 __global__ void __launch_bounds__(TS >= 32 ? TS : 32, (TS >= 64 && sizeof(L1) == 4) ? 5 : 1)
 team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
 {

@@ -129,8 +129,9 @@ struct RadauParams {
     double atol, rtol;
 };
 
-// LEARN: learned proposals and step records compiled in (block teams only)
-template <int N, int TS, class Mech, typename LT, class Store, bool LEARN = false>
+// LEARN (block teams only): 0 off; 1 step-size proposals and step records; 2 also
+// stage proposals (which hold three more state vectors per thread)
+template <int N, int TS, class Mech, typename LT, class Store, int LEARN = 0>
 struct Radau {
     using V = Vec<N, TS>;
     using TM = Team<TS>;
@@ -447,7 +448,8 @@ struct Radau {
                     TM::sync();
                     const float* o = mlp_infer_team<TS>(learn->mlp, xb, xb + MLP_D0, xb + MLP_D0 + MLP_D4);
                     const double Hp = Hprev * exp10(double(o[3 * N]));
-                    if (mlp_flags & MLP_USE_Z) {
+                    if constexpr (LEARN >= 2) {
+                      if (mlp_flags & MLP_USE_Z) {
 #pragma unroll
                         for (int s = 0; s < S; ++s) {
                             const int i = V::idx(s);
@@ -457,6 +459,7 @@ struct Radau {
                             ZP3[s] = V::ok(s) ? symexp(double(o[2 * N + i])) * si : 0.0;
                         }
                         have_zp = true;
+                      }
                     }
                     TM::sync();
                     if ((mlp_flags & MLP_USE_H) && Hp == Hp) {
@@ -499,8 +502,8 @@ struct Radau {
             double Fac = 0.5;
             int NewtonIter = 0;
             double Theta = 0;
-            for (int attempt = 0; attempt < 2; ++attempt) {
-            const bool use_zp = have_zp && attempt == 0;
+            for (int attempt = 0; attempt < (LEARN >= 2 ? 2 : 1); ++attempt) {
+            const bool use_zp = LEARN >= 2 && have_zp && attempt == 0;
             if (use_zp) {
 #pragma unroll
                 for (int s = 0; s < S; ++s) { Z1[s] = ZP1[s]; Z2[s] = ZP2[s]; Z3[s] = ZP3[s]; }
