@@ -32,7 +32,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_mlp_sizes", "accelerInt_mlp_forward", "accelerInt_mlp_loss_grad", "accelerInt_mlp_adam_step",
     "accelerInt_set_learned", "accelerInt_set_step_recording", "accelerInt_set_graph_launch",
     "accelerInt_set_launch_config", "accelerInt_autotune", "accelerInt_set_persistent",
-    "accelerInt_set_queue_order", "accelerInt_set_cost_model",
+    "accelerInt_set_queue_order", "accelerInt_set_cost_model", "accelerInt_set_learned_growth_floor",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -72,6 +72,7 @@ def load_library():
     lib.accelerInt_set_persistent.argtypes = [i]
     lib.accelerInt_set_queue_order.argtypes = [i]
     lib.accelerInt_set_cost_model.argtypes = [vp, vp]
+    lib.accelerInt_set_learned_growth_floor.argtypes = [ctypes.c_double]
     lib.accelerInt_set_launch_config.argtypes = [i, i]
     lib.accelerInt_autotune.argtypes = [i, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, i, vp, vp, vp]
     lib.accelerInt_kernel_launches.argtypes = []

@@ -653,6 +653,13 @@ int accelerInt_set_learned(const float* params_dev, const float* norm_dev, int f
     g.learn.mlp.p = params_dev;
     g.learn.mlp.norm = norm_dev;
     g.learn.mlp.flags = flags;
+    if (!(g.learn.mlp.growth_floor > 1.0)) g.learn.mlp.growth_floor = 2.0;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_learned_growth_floor(double floor) {
+    if (!(floor >= 1.05) || !(floor <= 8.0)) return ACCELERINT_ERR_ARGUMENT;
+    g.learn.mlp.growth_floor = floor;
     return ACCELERINT_OK;
 }
 

@@ -43,6 +43,7 @@ struct MlpDevice {
     const float* p;           // FP32 parameter vector (biases read from here)
     const float* norm;        // MLP_NNORM floats
     int flags;
+    double growth_floor;      // the step-size proposal never holds the step below this x the last accepted
 };
 __host__ __device__ constexpr int mlp_wq(int l) {   // offset of W_l in the bf16 weight block
     int o = 0;

@@ -442,7 +442,8 @@ struct Radau {
             if constexpr (LEARN) {
                 // the step-size proposal can only bind when the controller grows the
                 // step more than 2x; stage proposals are wanted on every step
-                if (mlp_flags && !Reject && ((mlp_flags & MLP_USE_Z) || H > 2.0 * Hprev)) {
+                const double gf = learn ? learn->mlp.growth_floor : 2.0;
+                if (mlp_flags && !Reject && ((mlp_flags & MLP_USE_Z) || H > gf * Hprev)) {
                     float* xb = reinterpret_cast<float*>(st.scratch_rhs());
                     mlp_features(y, Hprev, xb);
                     TM::sync();
@@ -464,9 +465,9 @@ struct Radau {
                     TM::sync();
                     if ((mlp_flags & MLP_USE_H) && Hp == Hp) {
                         // limits growth only: never above the controller's step, and
-                        // never below twice the last accepted one, so the proposal cannot
-                        // hold the step size down
-                        const double Hn = fmin(H, fmax(Hp, 2.0 * Hprev));
+                        // never below growth_floor (> 1) x the last accepted one, so the
+                        // proposal cannot hold the step size down
+                        const double Hn = fmin(H, fmax(Hp, gf * Hprev));
                         if (Hn != H) {
                             H = Hn;
                             SkipLU = false;

@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--no-graph", action="store_true")
     p.add_argument("--learned", type=int, default=1, choices=[0, 1, 2, 3],
                    help="learned proposals in the tuned form: 1 step size, 2 stages, 3 both (0: off)")
+    p.add_argument("--growth-floor", type=float, default=2.0,
+                   help="learned step-size proposals never hold the step below this x the last accepted")
     p.add_argument("--train-num", type=int, default=4096,
                    help="systems of the differently seeded batch whose plain Radau steps train the MLP")
     args = p.parse_args()
@@ -260,6 +262,8 @@ def run_ours(args):
     integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu)
     if model is not None:
         model.install(integ, args.learned)
+        integ.lib.accelerInt_set_learned_growth_floor(args.growth_floor)
+        learn_info["growth_floor"] = args.growth_floor
     if cost_model is not None:
         cost_model.install_cost(integ)
     stream = torch.cuda.Stream(device=dev)

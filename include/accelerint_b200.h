@@ -149,7 +149,7 @@ int accelerInt_get_poles(double* poles_re, double* poles_im, double* res_re, dou
  * kernels below compute with BF16-rounded weights and activations and FP32
  * accumulation.  norm holds in_mu[64] in_sd[64] out_mu[176] out_sd[176].
  * All pointers are device pointers; M (batch) must be a multiple of 16. */
-#define ACCELERINT_MLP_USE_H 1   /* limit step growth: min(controller, max(proposal, 2 x last accepted)) */
+#define ACCELERINT_MLP_USE_H 1   /* limit step growth: min(controller, max(proposal, floor x last accepted)) */
 #define ACCELERINT_MLP_USE_Z 2   /* start Newton from the proposed stages; on failure retry from the extrapolation */
 int accelerInt_mlp_sizes(int* nparam, int* nnorm, int* d_in, int* d_out);
 /* y[M x 176] = de-standardised network output for raw inputs x[M x 64] */
@@ -164,6 +164,9 @@ int accelerInt_mlp_adam_step(float* params_dev, const float* grad_dev, float* m_
 /* Install (flags != 0) or remove (flags == 0) the model for the mass-action Radau
  * kernels; the parameter and norm buffers must stay valid while installed. */
 int accelerInt_set_learned(const float* params_dev, const float* norm_dev, int flags);
+/* Growth floor of ACCELERINT_MLP_USE_H (default 2): the proposal limits the step to
+ * no less than floor x the last accepted step.  1.05 <= floor <= 8. */
+int accelerInt_set_learned_growth_floor(double floor);
 /* Capture one record per accepted Radau step (block teams): raw features [64] then
  * raw targets [176] -- symlog(Z_c,i / (atol + rtol |y_i|)) for c = 1..3, then
  * log10(H / H_previous) -- into rec_dev[capacity][240]; *count_dev counts records claimed (it may
