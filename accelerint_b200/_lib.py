@@ -33,6 +33,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_set_learned", "accelerInt_set_step_recording", "accelerInt_set_graph_launch",
     "accelerInt_set_launch_config", "accelerInt_autotune", "accelerInt_set_persistent",
     "accelerInt_set_queue_order", "accelerInt_set_cost_model", "accelerInt_set_learned_growth_floor",
+    "accelerInt_set_jacobian",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -70,6 +71,7 @@ def load_library():
     lib.accelerInt_set_step_recording.argtypes = [vp, vp, i]
     lib.accelerInt_set_graph_launch.argtypes = [i]
     lib.accelerInt_set_persistent.argtypes = [i]
+    lib.accelerInt_set_jacobian.argtypes = [i]
     lib.accelerInt_set_queue_order.argtypes = [i]
     lib.accelerInt_set_cost_model.argtypes = [vp, vp]
     lib.accelerInt_set_learned_growth_floor.argtypes = [ctypes.c_double]
@@ -162,6 +164,9 @@ class Integrator:
 
     def set_queue_order(self, mode: int):
         self._check(self.lib.accelerInt_set_queue_order(int(mode)))
+
+    def set_jacobian(self, finite_difference: bool):
+        self._check(self.lib.accelerInt_set_jacobian(1 if finite_difference else 0))
 
     def set_persistent(self, enable: bool = True):
         self._check(self.lib.accelerInt_set_persistent(1 if enable else 0))

@@ -80,6 +80,7 @@ struct State {
     int last_occ = 0;             // resident blocks per SM of the last team launch
     bool graph = false;           // device-buffer launches through a captured CUDA graph
     bool persistent = true;       // team kernels: persistent grid + work queue (else one team per system)
+    int jac_mode = 0;             // 0 analytic Jacobian, 1 finite differences (fd_jacob.c)
     int order_mode = 0;           // work-queue order: 0 index, 1 by y_0 (descending), 2 by last call's steps
     int order_cap = 0;            // systems the order buffers hold
     int* order_buf = nullptr;     // [order_cap] queue slot -> system
@@ -294,6 +295,16 @@ int launch_mass_action(BatchArgs a, cudaStream_t s) {
     M mech;
     const int R = g.mt.R;
     constexpr int N = M::N;
+    if (g.jac_mode == 1) {
+        // finite-difference Jacobian: plain FP64 Radau (the form of the reference's
+        // FINITE_DIFFERENCE build)
+        if (g.solver != ACCELERINT_RADAU2A || g.lu != ACCELERINT_LU_FP64) return ACCELERINT_ERR_UNSUPPORTED;
+        FdJacobian<M> fd;
+        fd.atol = g.atol;
+        fd.rtol = g.rtol;
+        TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
+        return launch_team<SK_RADAU, FdJacobian<M>, TS, double>(a, fd, lay, s);
+    }
     if (g.solver == ACCELERINT_RADAU2A) {
         // learned level: 2 with stage proposals, 1 with step-size proposals or records only
         const int learn = (a.learn.mlp.flags & MLP_USE_Z) ? 2 : (a.learn.rec != nullptr || a.learn.mlp.flags) ? 1 : 0;
@@ -325,6 +336,16 @@ int launch_mass_action(BatchArgs a, cudaStream_t s) {
 
 int launch_vdp(BatchArgs a, cudaStream_t s) {
     const int block = g.tps_block, grid = (a.num + block - 1) / block;
+    if (g.jac_mode == 1) {
+        if (g.solver != ACCELERINT_RADAU2A || g.lu != ACCELERINT_LU_FP64) return ACCELERINT_ERR_UNSUPPORTED;
+        FdJacobian<VanDerPol> fd;
+        fd.atol = g.atol;
+        fd.rtol = g.rtol;
+        tps_kernel<SK_RADAU, FdJacobian<VanDerPol>, double><<<grid, block, 0, s>>>(a, fd);
+        CK(cudaGetLastError());
+        g.launches++;
+        return ACCELERINT_OK;
+    }
     if (g.solver == ACCELERINT_RADAU2A) {
         if (g.lu == ACCELERINT_LU_FP32) tps_kernel<SK_RADAU, VanDerPol, float><<<grid, block, 0, s>>>(a, VanDerPol{});
         else tps_kernel<SK_RADAU, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
@@ -489,6 +510,7 @@ void accelerInt_cleanup(void) {
     g.tps_block = 128;
     g.graph = false;
     g.persistent = true;
+    g.jac_mode = 0;
     g.order_mode = 0;
     if (g.order_buf) cudaFree(g.order_buf);
     if (g.cost_buf) cudaFree(g.cost_buf);
@@ -672,6 +694,12 @@ int accelerInt_set_cost_model(const float* params_dev, const float* norm_dev) {
     if ((params_dev == nullptr) != (norm_dev == nullptr)) return ACCELERINT_ERR_ARGUMENT;
     g.cost_params = params_dev;
     g.cost_norm = norm_dev;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_jacobian(int mode) {
+    if (mode != 0 && mode != 1) return ACCELERINT_ERR_ARGUMENT;
+    g.jac_mode = mode;
     return ACCELERINT_OK;
 }
 

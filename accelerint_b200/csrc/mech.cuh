@@ -319,4 +319,45 @@ struct MassAction {
     }
 };
 
+// Finite-difference Jacobian over any mechanism's dydt (generic/fd_jacob.c with
+// FD_ORD 1): forward differences with increment r_j = max(sqrt(eps) |y_j|,
+// r0 / ewt_j), ewt = atol + rtol |y|, r0 = 1000 rtol eps N sqrt(sum (ewt dy)^2 / N)
+// -- the reference's weighting, kept for parity.  N + 1 dydt calls per Jacobian;
+// the owner of column j perturbs its element, every thread writes its rows.
+template <class Mech>
+struct FdJacobian : Mech {
+    static constexpr int N = Mech::N;
+    double atol, rtol;
+    template <int TS>
+    __device__ __noinline__ void jacob(double t, double P, const Vec<N, TS>& y, double* J, double* sm) const {
+        using V = Vec<N, TS>;
+        using TM = Team<TS>;
+        V dy, yp, ft;
+        Mech::template dydt<TS>(t, P, y, dy, sm);
+        double ewt[V::S], sum = 0.0;
+#pragma unroll
+        for (int s = 0; s < V::S; ++s) {
+            ewt[s] = atol + rtol * fabs(y[s]);
+            if (V::ok(s)) sum += (ewt[s] * dy[s]) * (ewt[s] * dy[s]);
+        }
+        const double fac = sqrt(TM::sum(sum) / double(N));
+        const double r0 = 1000.0 * rtol * DBL_EPSILON * double(N) * fac;
+        const double srur = sqrt(DBL_EPSILON);
+        for (int j = 0; j < N; ++j) {
+            double rj = 0.0;
+#pragma unroll
+            for (int s = 0; s < V::S; ++s)
+                if (V::idx(s) == j) rj = fmax(srur * fabs(y[s]), r0 / ewt[s]);
+            const double r = TM::bcast(rj, j % TS);
+#pragma unroll
+            for (int s = 0; s < V::S; ++s) yp[s] = (V::idx(s) == j) ? y[s] + r : y[s];
+            Mech::template dydt<TS>(t, P, yp, ft, sm);
+#pragma unroll
+            for (int s = 0; s < V::S; ++s)
+                if (V::ok(s)) J[V::idx(s) + N * j] = (ft[s] - dy[s]) / r;
+        }
+        TM::sync();
+    }
+};
+
 }  // namespace aib

@@ -201,6 +201,10 @@ int accelerInt_set_graph_launch(int enable);
  * the plain form, one team per system over a grid of NUM teams (one Jacobian
  * scratch per system). */
 int accelerInt_set_persistent(int enable);
+/* Jacobian of the mechanism: 0 analytic (default); 1 first-order finite
+ * differences over dydt with the increments of generic/fd_jacob.c (the
+ * reference's FINITE_DIFFERENCE build), for plain FP64 Radau. */
+int accelerInt_set_jacobian(int mode);
 int accelerInt_set_queue_order(int mode);
 int accelerInt_set_cost_model(const float* params_dev, const float* norm_dev);
 int accelerInt_set_launch_config(int occupancy_cap, int tps_block);

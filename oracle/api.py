@@ -24,7 +24,8 @@ class _Mech(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("n", ctypes.c_int), ("n_species", ctypes.c_int),
                 ("n_reactions", ctypes.c_int), ("mw", _dp), ("cp", _dp), ("h_form", _dp),
                 ("s_ref", _dp), ("log_a", _dp), ("beta", _dp), ("ta", _dp), ("reac", _ip),
-                ("prod", _ip)]
+                ("prod", _ip), ("jac_fd", ctypes.c_int), ("fd_atol", ctypes.c_double),
+                ("fd_rtol", ctypes.c_double)]
 
 
 class _Config(ctypes.Structure):
@@ -56,10 +57,13 @@ def reference_available(solver: str = "radau2a", n: int = 2) -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", f"libref_{solver}_n{n}.so"))
 
 
-def _mech_struct(mech, keep):
+def _mech_struct(mech, keep, fd=None):
+    """fd: (atol, rtol) for a finite-difference Jacobian (generic/fd_jacob.c), else None."""
     from accelerint_b200.mechanism import MECH_VAN_DER_POL
     m = _Mech()
     m.n = mech.n_state
+    if fd is not None:
+        m.jac_fd, m.fd_atol, m.fd_rtol = 1, fd[0], fd[1]
     if mech.kind == MECH_VAN_DER_POL:
         m.kind = 0
         return m
@@ -118,10 +122,11 @@ class Oracle:
             c.res_re[i], c.res_im[i] = r[i].real, r[i].imag
         return c
 
-    def integrate(self, solver, mech, y, var, t0, t1, atol=1e-10, rtol=1e-6, nthreads=0, poles=None):
+    def integrate(self, solver, mech, y, var, t0, t1, atol=1e-10, rtol=1e-6, nthreads=0, poles=None,
+                  fd_jacobian=False):
         """One global step [t0, t1] for every system.  Returns (y_new, codes, stats[num, NSTATS])."""
         keep = []
-        m = _mech_struct(mech, keep)
+        m = _mech_struct(mech, keep, (atol, rtol) if fd_jacobian else None)
         c = self.config(atol, rtol, poles)
         y = np.array(y, dtype=np.float64, order="C", copy=True)
         num = y.shape[1]
@@ -151,10 +156,11 @@ class Oracle:
         self.lib.or_dydt(ctypes.byref(m), t, var, y.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
         return out
 
-    def jacob(self, mech, y, var, t=0.0):
-        """Column-major Jacobian returned as an [N, N] array J[i, j] = d f_i / d y_j."""
+    def jacob(self, mech, y, var, t=0.0, fd=None):
+        """Column-major Jacobian returned as an [N, N] array J[i, j] = d f_i / d y_j
+        (fd = (atol, rtol): by finite differences, generic/fd_jacob.c)."""
         keep = []
-        m = _mech_struct(mech, keep)
+        m = _mech_struct(mech, keep, fd)
         y = np.ascontiguousarray(y, dtype=np.float64)
         n = y.shape[0]
         out = np.zeros(n * n)
@@ -198,6 +204,15 @@ class Reference:
         self.lib.ref_int_driver.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp,
                                             ctypes.c_int]
         self.lib.ref_poles.argtypes = [_dp, _dp, _dp, _dp]
+        if solver == "radau2a":
+            self.lib.ref_fd_eval_jacob.argtypes = [ctypes.c_double, ctypes.c_double, _dp, _dp]
+
+    def fd_jacob(self, y, pres, t=0.0):
+        """The reference's generic/fd_jacob.c (ATOL 1e-10, RTOL 1e-6) at one state: [N, N]."""
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros(self.n * self.n)
+        self.lib.ref_fd_eval_jacob(t, pres, y.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
+        return out.reshape(self.n, self.n, order="F")
         self._keep = []
         self.lib.ref_init()
 

@@ -9,6 +9,8 @@
  *              generated code is absent from the reference repository).
  */
 #include <math.h>
+#include <float.h>
+#include <string.h>
 #include <string.h>
 #include "oracle.h"
 
@@ -207,8 +209,37 @@ void or_dydt(const or_mech* m, double t, double pr, const double* y, double* dy)
     else ma_dydt(m, pr, y, dy);
 }
 
+/* generic/fd_jacob.c:24-127 with FD_ORD 1: forward differences, increment
+ * r_j = max(sqrt(eps) |y_j|, r0 / ewt_j), ewt = ATOL + RTOL |y|,
+ * r0 = 1000 RTOL eps N sqrt(sum (ewt dy)^2 / N). */
+static void fd_jacob(const or_mech* m, double t, double pr, const double* cy, double* jac)
+{
+    const int n = m->n;
+    double y[OR_NMAX], dy[OR_NMAX], ftemp[OR_NMAX], ewt[OR_NMAX];
+    memcpy(y, cy, n * sizeof(double));
+    or_dydt(m, t, pr, y, dy);
+    for (int i = 0; i < n; ++i) ewt[i] = m->fd_atol + (m->fd_rtol * fabs(y[i]));
+    const double srur = sqrt(DBL_EPSILON);
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i) sum += (ewt[i] * dy[i]) * (ewt[i] * dy[i]);
+    const double fac = sqrt(sum / ((double)(n)));
+    const double r0 = 1000.0 * m->fd_rtol * DBL_EPSILON * ((double)(n)) * fac;
+    for (int j = 0; j < n; ++j) {
+        const double yj_orig = y[j];
+        const double r = fmax(srur * fabs(yj_orig), r0 / ewt[j]);
+        y[j] = yj_orig + r;
+        or_dydt(m, t, pr, y, ftemp);
+        for (int i = 0; i < n; ++i) jac[i + n * j] = (ftemp[i] - dy[i]) / r;
+        y[j] = yj_orig;
+    }
+}
+
 void or_jacob(const or_mech* m, double t, double pr, const double* y, double* jac)
 {
+    if (m->jac_fd) {
+        fd_jacob(m, t, pr, y, jac);
+        return;
+    }
     (void)t;
     if (m->kind == OR_MECH_VDP) vdp_jacob(pr, y, jac);
     else ma_jacob(m, pr, y, jac);

@@ -41,6 +41,8 @@ typedef struct {
     int n_species, n_reactions;
     const double *mw, *cp, *h_form, *s_ref, *log_a, *beta, *ta;
     const int *reac, *prod;   /* [R*2], -1 = empty slot */
+    int jac_fd;               /* 1: Jacobian by first-order finite differences (generic/fd_jacob.c) */
+    double fd_atol, fd_rtol;  /* the ATOL / RTOL the difference increments use */
 } or_mech;
 
 typedef struct {
