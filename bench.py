@@ -76,6 +76,8 @@ def parse():
                    help="learned proposals in the tuned form: 1 step size, 2 stages, 3 both (0: off)")
     p.add_argument("--growth-floor", type=float, default=2.0,
                    help="learned step-size proposals never hold the step below this x the last accepted")
+    p.add_argument("--train-epochs", type=int, default=8)
+    p.add_argument("--train-batch", type=int, default=4096)
     p.add_argument("--train-num", type=int, default=4096,
                    help="systems of the differently seeded batch whose plain Radau steps train the MLP")
     args = p.parse_args()
@@ -247,7 +249,8 @@ def run_ours(args):
         t0 = time.time()
         yt, vt = M.mixed_stiffness_initial_conditions(mech, args.train_num, args.seed + 104729 + rank)
         rec = Lm.record_steps(mech, yt, vt, 0.0, args.steps * DT, DT, capacity=1 << 22, device=dev.index)
-        model = Lm.train(rec, mech.n_state, epochs=8, batch=4096, lr=2e-3)
+        model = Lm.train(rec, mech.n_state, epochs=args.train_epochs, batch=args.train_batch,
+                         lr=2e-3 if args.train_batch >= 4096 else 1e-3)
         learn_info = {"flags": args.learned, "train_systems": args.train_num, "records": int(rec.shape[0]),
                       "holdout_loss": model.history[-1], "train_s": time.time() - t0}
         del rec
