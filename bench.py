@@ -13,7 +13,7 @@ conditions, then the state is reset), so the transient after t = 0 is always
 inside the timed region.  L2 is flushed (a 256 MiB write) between timed steps,
 outside the per-step event pairs.
 
-The tuned form is the three north-star changes on top of the plain FP64 form:
+The tuned form is three changes on top of the plain FP64 form:
 E1/E2 factorised and solved in FP32 (--lu), the persistent work-queue kernel
 under a captured CUDA graph with the autotuned mapping and a longest-first
 queue order from a learned per-system cost model (--queue-order 3), and the
@@ -122,11 +122,12 @@ class ClockSampler:
     def __init__(self, index=0):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="accelerint_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
@@ -149,7 +150,9 @@ class ClockSampler:
 
     def summary(self):
         try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            with open(self.path) as f:
+                rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
+            os.remove(self.path)
         except Exception:
             rows = []
         if not rows:

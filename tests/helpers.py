@@ -5,7 +5,7 @@ sequences are sensitive to the last bit: the reference CPU solver itself,
 given initial conditions perturbed by 1e-15 relative, ends some systems with
 different step counts and final states that differ by up to ~1e-3 relative.
 GPU-vs-CPU parity is therefore checked as
-  (1) the share of systems that agree to the north-star tolerance (weighted
+  (1) the share of systems that agree to the parity tolerance (weighted
       error < 1, i.e. |x - x_ref| < atol + rtol |x_ref| with rtol 1e-6, atol
       1e-10) is at least the share the perturbed reference reaches, less 0.1, and
   (2) the worst system differs no more than the reference differs from itself
