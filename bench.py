@@ -184,10 +184,10 @@ def cpu_baseline(args, mech, y, var):
     sys.path.insert(0, ROOT)
     from oracle import Reference, reference_available, Oracle, oracle_available
     nthreads = os.cpu_count() or 1
-    # 48 systems per thread: the first three 53-species global steps cost ~0.2 s per
-    # system on one core, so the sample takes ~10 s whatever the core count, and
+    # 128 systems per thread: the first three 53-species global steps cost ~0.08 s
+    # per system on one core, so the sample takes ~10 s whatever the core count, and
     # holds enough of the few very stiff systems for a stable rate
-    sample = args.cpu_sample or min(args.num, 8192, 48 * nthreads)
+    sample = args.cpu_sample or min(args.num, 16384, 128 * nthreads)
     ys, vs = y[:, :sample].copy(), var[:sample].copy()
     if reference_available("radau2a", 54):
         ref = Reference("radau2a", 54)
