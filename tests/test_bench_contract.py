@@ -1,0 +1,48 @@
+"""bench.py's reference arm runs on the CPU (the reference's own radau2a.c, or
+the oracle port) and prints the one JSON line of the bench contract."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_contract_line():
+    from oracle import oracle_available, reference_available
+    if not (reference_available("radau2a", 54) or oracle_available()):
+        pytest.skip("neither the reference build nor the oracle is built")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1", "--cpu-sample", "4"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+
+
+def test_flop_model_counts_events():
+    sys.path.insert(0, ROOT)
+    import bench
+    st = np.zeros((2, 10))
+    st[0, 4] = 1          # one factorisation at N = 54
+    f = bench.flops_per_system(st)
+    assert f[1] == 0.0
+    assert abs(f[0] - ((2.0 / 3.0 + 8.0 / 3.0) * 54 ** 3 + 54 * 54)) < 1e-6
+
+
+def test_state_features_layout():
+    import accelerint_b200 as A
+    from accelerint_b200 import learned as L
+    mech = A.mechanism_13()
+    y, var = A.mass_action_initial_conditions(mech, 5, seed=2)
+    x = L.state_features(y, var, 1e-6)
+    assert x.shape == (5, L.D_IN)
+    assert np.allclose(x[:, 0], y[0]) and np.allclose(x[:, 14], -6.0) and np.allclose(x[:, 15], 0.0)
+    assert (x[:, 16:] == 0).all()
