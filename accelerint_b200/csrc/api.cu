@@ -16,6 +16,7 @@ namespace aib_cf {
 int poles_residues(int n, double atol, double* pr, double* pi, double* rr, double* ri);
 }
 namespace aib_mlp {
+void free_work();
 int to_bf16(const float* params, void* w_bf16, cudaStream_t s);
 int predict_cost(const float* params, const float* norm, int num, int n, const double* y, const double* var,
                  double h, float* x, float* out, float* key, cudaStream_t s);
@@ -502,6 +503,7 @@ void accelerInt_cleanup(void) {
     if (g.queue) cudaFree(g.queue);
     if (g.mlp_w) cudaFree(g.mlp_w);
     g.mlp_w = nullptr;
+    aib_mlp::free_work();
     if (g.gexec) cudaGraphExecDestroy(g.gexec);
     g.gexec = nullptr;
     if (g.cap_stream) cudaStreamDestroy(g.cap_stream);

@@ -240,6 +240,12 @@ __global__ void column0_kernel(int num, const float* y, float* key) {
 }  // namespace
 
 namespace aib_mlp {
+// release the activation / gradient workspace (accelerInt_cleanup)
+void free_work() {
+    if (g_work.buf) cudaFree(g_work.buf);
+    g_work = Work{};
+}
+
 // bf16 copy of the weights for the solver (api.cu)
 int to_bf16(const float* params, void* w_bf16, cudaStream_t s) {
     to_bf16_kernel<<<nblk(MLP_NWEIGHT), 256, 0, s>>>(params, static_cast<__nv_bfloat16*>(w_bf16));
