@@ -1,6 +1,9 @@
 // C-ABI of libaccelerint_b200.so: the reference's accelerInt_initialize /
 // accelerInt_integrate / accelerInt_cleanup (generic/solver_interface.cu:88-225)
-// plus run-time selection of solver, mechanism, tolerances and precision.
+// plus run-time selection of solver, mechanism, Jacobian, tolerances and
+// precision, the device-buffer / graph / allocation-free entry points, the
+// launch mapping (persistent queue, queue order, autotuner) and the learned
+// proposals.  One process-wide instance, as in the reference.
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstring>

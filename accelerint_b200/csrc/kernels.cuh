@@ -7,7 +7,10 @@
 //   * persistent team kernels for the mass-action mechanisms: one team of TS
 //     lanes per system, its matrices in shared memory; teams pull systems from
 //     a device work queue (one atomic per system), so systems with very
-//     different stiffness do not hold each other up.
+//     different stiffness do not hold each other up.  The queue can be taken
+//     in a longest-first order (a counting sort of per-system cost keys,
+//     order_*_kernel below) so that the launch does not end on one stiff
+//     system; a plain-grid mode (one team per system) is the plain form.
 // Every kernel integrates all global steps [t_k, t_{k+1}] of its systems in
 // one launch; each step restarts the integrator exactly as a separate
 // intDriver call of the reference would.

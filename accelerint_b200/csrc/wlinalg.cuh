@@ -1,6 +1,8 @@
-// Warp-level dense LU factorisation and solves for block teams: one warp per
-// matrix (32 lanes, rows i = lane + 32 r), the matrix column-major in shared
-// memory.  In a two-warp team warp 0 works on E1 while warp 1 works on E2.
+// Warp-level dense LU factorisation and solves for block teams: rows
+// i = lane + 32 r of a column-major matrix in shared memory.  A 32-thread team
+// factors E1 and E2 on its one warp (wlu_real / wlu_cplx); a 64-thread team
+// factors both overlapped on its two warps (tlu_pair).  Solves run E1 on warp 0
+// and E2 on warp 1 (wsolve_real / wsolve_cplx), in the factors' precision.
 //
 // Semantics of LAPACK's unblocked xGETF2 / xGETRS as in linalg.cuh (first
 // maximal pivot by |a| or |Re a| + |Im a|, reciprocal scaling of the
