@@ -65,3 +65,59 @@ def test_kernel_launch_counter_is_exported():
     lib = _lib()
     lib.accelerInt_kernel_launches.restype = ctypes.c_longlong
     assert lib.accelerInt_kernel_launches() >= 0
+
+
+def test_extension_setters_validate_without_a_device():
+    import ctypes
+    lib = _lib()
+    # queue order 3 needs a cost model; orders outside 0..3 are rejected
+    lib.accelerInt_set_cost_model(None, None)
+    assert lib.accelerInt_set_queue_order(3) == -3
+    assert lib.accelerInt_set_queue_order(4) == -1
+    assert lib.accelerInt_set_queue_order(0) == 0
+    # growth floor bounds, Jacobian modes, launch configuration
+    lib.accelerInt_set_learned_growth_floor.argtypes = [ctypes.c_double]
+    assert lib.accelerInt_set_learned_growth_floor(1.0) == -1
+    assert lib.accelerInt_set_learned_growth_floor(9.0) == -1
+    assert lib.accelerInt_set_learned_growth_floor(2.0) == 0
+    assert lib.accelerInt_set_jacobian(2) == -1
+    assert lib.accelerInt_set_jacobian(0) == 0
+    assert lib.accelerInt_set_launch_config(-1, 0) == -1
+    assert lib.accelerInt_set_launch_config(0, 48) == -1
+    # learned proposals: unknown flags, missing buffers, not initialised
+    assert lib.accelerInt_set_learned(None, None, 4) == -1
+    assert lib.accelerInt_set_learned(None, None, 1) == -1
+    assert lib.accelerInt_set_learned(None, None, 0) == 0
+    assert lib.accelerInt_set_step_recording(ctypes.c_void_p(16), None, 10) == -1
+    assert lib.accelerInt_set_step_recording(None, None, 0) == 0
+
+
+def test_entry_points_refuse_before_initialize():
+    import ctypes
+    lib = _lib()
+    lib.accelerInt_cleanup()
+    dp = ctypes.POINTER(ctypes.c_double)
+    import numpy as np
+    y = np.zeros((2, 4))
+    var = np.ones(4)
+    assert lib.accelerInt_integrate_status(4, 0.0, 1.0, 0.1, y.ctypes.data_as(dp), var.ctypes.data_as(dp)) == -3
+    vp = ctypes.c_void_p
+    lib.accelerInt_integrate_device.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                vp, vp, vp, vp, vp]
+    assert lib.accelerInt_integrate_device(4, 0.0, 1.0, 0.1, vp(16), vp(16), None, None, None) == -3
+    lib.accelerInt_integrate_device_noalloc.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_double, vp, vp, vp, vp]
+    assert lib.accelerInt_integrate_device_noalloc(4, 0.0, 1.0, 0.1, vp(16), vp(16), None, None) == -3
+    lib.accelerInt_autotune.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp,
+                                        ctypes.c_int, vp, vp, vp]
+    assert lib.accelerInt_autotune(4, 0.0, 1.0, 0.1, vp(16), vp(16), 4, None, None, None) == -3
+
+
+def test_mlp_sizes_match_the_python_layout():
+    import ctypes
+    from accelerint_b200 import learned as L
+    lib = _lib()
+    a = [ctypes.c_int() for _ in range(4)]
+    lib.accelerInt_mlp_sizes.argtypes = [ctypes.c_void_p] * 4
+    assert lib.accelerInt_mlp_sizes(*[ctypes.byref(x) for x in a]) == 0
+    assert [x.value for x in a] == [L.n_params(), 2 * L.D_IN + 2 * L.D_OUT, L.D_IN, L.D_OUT]
