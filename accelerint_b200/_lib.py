@@ -16,6 +16,7 @@ ACCELERINT_ERR_CUDA = -2
 ACCELERINT_ERR_STATE = -3
 ACCELERINT_ERR_UNSUPPORTED = -4
 ACCELERINT_ERR_SYSTEMS = -5
+ACCELERINT_EC_NONFINITE = 5   # per-system code: success reported but the final state is not finite
 SOLVERS = {"radau2a": 0, "exprb43": 1, "exp4": 2, "rkc": 3}
 LU_FP64, LU_FP32, LU_FP32_ALL = 0, 1, 2
 NSTATS = 10
@@ -33,7 +34,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_set_learned", "accelerInt_set_step_recording", "accelerInt_set_graph_launch",
     "accelerInt_set_launch_config", "accelerInt_autotune", "accelerInt_set_persistent",
     "accelerInt_set_queue_order", "accelerInt_set_cost_model", "accelerInt_set_learned_growth_floor",
-    "accelerInt_set_jacobian",
+    "accelerInt_set_jacobian", "accelerInt_radau_decomp",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -77,6 +78,7 @@ def load_library():
     lib.accelerInt_set_learned_growth_floor.argtypes = [ctypes.c_double]
     lib.accelerInt_set_launch_config.argtypes = [i, i]
     lib.accelerInt_autotune.argtypes = [i, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, i, vp, vp, vp]
+    lib.accelerInt_radau_decomp.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, vp]
     lib.accelerInt_kernel_launches.argtypes = []
     lib.accelerInt_kernel_launches.restype = ctypes.c_longlong
     lib.accelerInt_set_mechanism_van_der_pol.argtypes = []

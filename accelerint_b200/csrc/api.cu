@@ -28,6 +28,23 @@ int predict_cost(const float* params, const float* norm, int num, int n, const d
 namespace {
 
 // FMA throughput probe: 8 independent dependency chains per thread.
+__device__ __forceinline__ float2 fma_probe(float2 a, float2 m, float2 c) { return __ffma2_rn(a, m, c); }
+__device__ __forceinline__ float fma_probe(float a, float m, float c) { return fmaf(a, m, c); }
+__device__ __forceinline__ double fma_probe(double a, double m, double c) { return fma(a, m, c); }
+__global__ void fma_peak_kernel2(float2* out, int iters, float2 m) {
+    float2 a[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = make_float2(float(threadIdx.x + c) * 1e-3f, float(c) * 1e-3f);
+    const float2 d = make_float2(1e-7f, 1e-7f);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a[c] = fma_probe(a[c], m, d);
+    }
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) { s.x += a[c].x; s.y += a[c].y; }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
 template <typename T>
 __global__ void fma_peak_kernel(T* out, int iters, T m) {
     T a[8];
@@ -100,6 +117,9 @@ struct State {
 };
 
 State g;
+
+constexpr int kMaxDevices = 64;
+void noalloc_forget();   // allocation-free entry point: drops its cached scratch addresses
 
 #define CK(x)                                                                                  \
     do {                                                                                       \
@@ -351,7 +371,11 @@ int launch_vdp(BatchArgs a, cudaStream_t s) {
         return ACCELERINT_OK;
     }
     if (g.solver == ACCELERINT_RADAU2A) {
-        if (g.lu == ACCELERINT_LU_FP32) tps_kernel<SK_RADAU, VanDerPol, float><<<grid, block, 0, s>>>(a, VanDerPol{});
+        // E2 in FP32 (E1 in FP64), or both in FP32
+        if (g.lu == ACCELERINT_LU_FP32)
+            tps_kernel<SK_RADAU, VanDerPol, float, double><<<grid, block, 0, s>>>(a, VanDerPol{});
+        else if (g.lu == ACCELERINT_LU_FP32_ALL)
+            tps_kernel<SK_RADAU, VanDerPol, float, float><<<grid, block, 0, s>>>(a, VanDerPol{});
         else tps_kernel<SK_RADAU, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
     } else if (g.solver == ACCELERINT_RKC) {
         tps_kernel<SK_RKC, VanDerPol, double><<<grid, block, 0, s>>>(a, VanDerPol{});
@@ -363,6 +387,28 @@ int launch_vdp(BatchArgs a, cudaStream_t s) {
     CK(cudaGetLastError());
     g.launches++;
     return ACCELERINT_OK;
+}
+
+template <int K, int TS, typename LT, typename L1>
+int launch_decomp(int count, const double* jac, const double* h, void* e1, void* e2, int* perm, int* info,
+                  cudaStream_t s) {
+    using M = MassAction<K>;
+    constexpr int N = M::N;
+    const TeamLayout lay = TeamLayout::radau(N, int(sizeof(LT)), M::smem_rhs(0), M::smem_jac(0), int(sizeof(L1)));
+    auto kern = decomp_kernel<M, TS, LT, L1>;
+    if (lay.total > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
+    kern<<<count, TS, lay.total, s>>>(count, jac, h, static_cast<L1*>(e1), static_cast<cx<LT>*>(e2), perm, info, lay);
+    CK(cudaGetLastError());
+    g.launches++;
+    return ACCELERINT_OK;
+}
+
+template <int K, int TS>
+int launch_decomp_prec(int precision, int count, const double* jac, const double* h, void* e1, void* e2, int* perm,
+                       int* info, cudaStream_t s) {
+    if (precision == ACCELERINT_LU_FP64) return launch_decomp<K, TS, double, double>(count, jac, h, e1, e2, perm, info, s);
+    if (precision == ACCELERINT_LU_FP32) return launch_decomp<K, TS, float, double>(count, jac, h, e1, e2, perm, info, s);
+    return launch_decomp<K, TS, float, float>(count, jac, h, e1, e2, perm, info, s);
 }
 
 int launch(BatchArgs a, cudaStream_t s) {
@@ -469,6 +515,7 @@ extern "C" {
 
 void accelerInt_initialize(int NUM, int device) {
     g.last_status = ACCELERINT_OK;
+    noalloc_forget();
     device = device < 0 ? 0 : device;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device >= ndev) {
@@ -499,6 +546,7 @@ void accelerInt_integrate(const int NUM, const double t_start, const double t_en
 }
 
 void accelerInt_cleanup(void) {
+    noalloc_forget();
     if (g.y_dev) cudaFree(g.y_dev);
     if (g.var_dev) cudaFree(g.var_dev);
     if (g.codes_dev) cudaFree(g.codes_dev);
@@ -664,6 +712,23 @@ int accelerInt_get_poles(double* pr, double* pi, double* rr, double* ri) {
 }
 
 long long accelerInt_kernel_launches(void) { return g.launches; }
+
+int accelerInt_radau_decomp(int n, int precision, int count, const double* jac_dev, const double* h_dev,
+                            void* e1_dev, void* e2_dev, int* perm_dev, int* info_dev, void* stream) {
+    if (count < 0 || (count > 0 && (!jac_dev || !h_dev || !e1_dev || !e2_dev || !perm_dev || !info_dev)))
+        return ACCELERINT_ERR_ARGUMENT;
+    if (precision != ACCELERINT_LU_FP64 && precision != ACCELERINT_LU_FP32 && precision != ACCELERINT_LU_FP32_ALL)
+        return ACCELERINT_ERR_ARGUMENT;
+    if (count == 0) return ACCELERINT_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (n) {
+        case 14: return launch_decomp_prec<13, 32>(precision, count, jac_dev, h_dev, e1_dev, e2_dev, perm_dev,
+                                                   info_dev, s);
+        case 54: return launch_decomp_prec<53, 64>(precision, count, jac_dev, h_dev, e1_dev, e2_dev, perm_dev,
+                                                   info_dev, s);
+        default: return ACCELERINT_ERR_UNSUPPORTED;
+    }
+}
 
 int accelerInt_set_learned(const float* params_dev, const float* norm_dev, int flags) {
     if (flags & ~(ACCELERINT_MLP_USE_H | ACCELERINT_MLP_USE_Z)) return ACCELERINT_ERR_ARGUMENT;
@@ -837,6 +902,7 @@ int accelerInt_measure_fma_peak(int fp64, double* tflops) {
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     void* out = nullptr;
     const int block = 256, grid = sms * 8, iters = 4096;
+    if (fp64 < 0 || fp64 > 2) return ACCELERINT_ERR_ARGUMENT;
     CK(cudaMalloc(&out, size_t(grid) * block * sizeof(double)));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -844,7 +910,9 @@ int accelerInt_measure_fma_peak(int fp64, double* tflops) {
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         cudaEventRecord(e0);
-        if (fp64) fma_peak_kernel<double><<<grid, block>>>(static_cast<double*>(out), iters, 1.0000001);
+        if (fp64 == 1) fma_peak_kernel<double><<<grid, block>>>(static_cast<double*>(out), iters, 1.0000001);
+        else if (fp64 == 2)
+            fma_peak_kernel2<<<grid, block>>>(static_cast<float2*>(out), iters, make_float2(1.0000001f, 0.9999999f));
         else fma_peak_kernel<float><<<grid, block>>>(static_cast<float*>(out), iters, 1.0000001f);
         cudaEventRecord(e1);
         cudaEventSynchronize(e1);
@@ -856,7 +924,8 @@ int accelerInt_measure_fma_peak(int fp64, double* tflops) {
     cudaEventDestroy(e1);
     cudaFree(out);
     CK(cudaGetLastError());
-    const double flops = 2.0 * 8.0 * double(iters) * grid * block;   // 8 independent chains per thread
+    // 8 independent chains per thread; a packed FP32x2 FMA is two FMAs
+    const double flops = 2.0 * 8.0 * double(iters) * grid * block * (fp64 == 2 ? 2.0 : 1.0);
     *tflops = flops / (best * 1e-3) / 1e12;
     return ACCELERINT_OK;
 }
@@ -874,8 +943,14 @@ constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;   // 16 MiB
 constexpr size_t kNoAllocQueueBytes = 256;                   // queue counter + padding
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
 void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Forget the cached device addresses: after a device reset (the reference's
+// solver_interface.cu:111,224 calls cudaDeviceReset) the module, and with it the
+// array, may be loaded again at another address.
+void noalloc_forget() {
+    for (int d = 0; d < kMaxDevices; ++d) g_noalloc_ptr[d] = nullptr;
+}
 
 // Device address of the array for the current device, looked up once per device.
 // In host code the array's name is only a host-side stand-in, never a device address.
@@ -933,6 +1008,18 @@ int launch_mass_action_noalloc(BatchArgs a, unsigned char* scratch, cudaStream_t
     const int R = g.mt.R;
     constexpr int N = M::N;
     if (g.solver != ACCELERINT_RADAU2A) return ACCELERINT_ERR_UNSUPPORTED;
+    // learned proposals and step recording have no allocation-free kernels: refuse
+    // rather than integrate differently from accelerInt_integrate_device
+    if (g.learn.mlp.flags != 0 || g.learn.rec != nullptr) return ACCELERINT_ERR_UNSUPPORTED;
+    if (g.jac_mode == 1) {
+        // finite-difference Jacobian, as the allocating entry point runs it: plain FP64 only
+        if (g.lu != ACCELERINT_LU_FP64) return ACCELERINT_ERR_UNSUPPORTED;
+        FdJacobian<M> fd;
+        fd.atol = g.atol;
+        fd.rtol = g.rtol;
+        TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
+        return launch_team_noalloc<SK_RADAU, FdJacobian<M>, TS, double>(a, fd, lay, scratch, s);
+    }
     if (g.lu == ACCELERINT_LU_FP32) {
         TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 8);
         return launch_team_noalloc<SK_RADAU, M, TS, float, double>(a, mech, lay, scratch, s);

@@ -15,6 +15,9 @@ enum : int {
     EC_max_steps_exceeded = 2,
     EC_h_plus_t_equals_h = 3,
     EC_newton_max_iterations_exceeded = 4,
+    // not a reference code: the integrator reported success but the final state
+    // holds a NaN or an infinity (the reference returns 0 for such a system)
+    EC_nonfinite_state = 5,
 };
 
 // Per-system counters (stats_dev[ivp * NSTATS + k]).

@@ -66,7 +66,7 @@ __device__ __forceinline__ void store_stats(const BatchArgs& a, int sys, const S
 // ------------------------------------------------------------- thread per system
 enum SolverKind { SK_RADAU = 0, SK_EXPRB43 = 1, SK_EXP4 = 2, SK_RKC = 3 };
 
-template <int SK, class Mech, typename LT>
+template <int SK, class Mech, typename LT, typename L1 = LT>
 __global__ void __launch_bounds__(128) tps_kernel(BatchArgs a, Mech mech)
 {
     constexpr int N = Mech::N;
@@ -81,8 +81,8 @@ __global__ void __launch_bounds__(128) tps_kernel(BatchArgs a, Mech mech)
     int code = EC_success;
     StepLoop L(a.t_start, a.t_end, a.step);
     if constexpr (SK == SK_RADAU) {
-        RadauRegStore<N, LT> store;
-        Radau<N, 1, Mech, LT, RadauRegStore<N, LT>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
+        RadauRegStore<N, LT, L1> store;
+        Radau<N, 1, Mech, LT, RadauRegStore<N, LT, L1>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
         while (L.more() && code == EC_success) {
             code = rad.integrate(L.t, L.t_next, y);
             L.advance();
@@ -95,7 +95,10 @@ __global__ void __launch_bounds__(128) tps_kernel(BatchArgs a, Mech mech)
         }
     }
 #pragma unroll
-    for (int i = 0; i < N; ++i) a.y[size_t(i) * a.num + sys] = y[i];
+    for (int i = 0; i < N; ++i) {
+        a.y[size_t(i) * a.num + sys] = y[i];
+        if (code == EC_success && !isfinite(y[i])) code = EC_nonfinite_state;
+    }
     if (a.codes) a.codes[sys] = code;
     store_stats<N, 1>(a, sys, st);
 }
@@ -205,7 +208,8 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             store.rhs = reinterpret_cast<double*>(base + lay.rhs);
             store.inf = reinterpret_cast<int*>(base + lay.inf);
             const LearnArgs la = a.learn;
-            Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>, LEARN> rad{mech, store, RadauParams{a.atol, a.rtol},
+            Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>, LEARN> rad{mech, store,
+                                                                         RadauParams{a.atol, a.rtol},
                                                                          pr, st, LEARN ? &la : nullptr};
             while (L.more() && code == EC_success) {
                 code = rad.integrate(L.t, L.t_next, y);
@@ -237,13 +241,71 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
                 L.advance();
             }
         }
+        double bad = 0.0;
 #pragma unroll
         for (int s = 0; s < Vec<N, TS>::S; ++s)
-            if (Vec<N, TS>::ok(s)) a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] = y[s];
+            if (Vec<N, TS>::ok(s)) {
+                a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] = y[s];
+                if (!isfinite(y[s])) bad = 1.0;
+            }
+        if (code == EC_success && TM::sum(bad) > 0.0) code = EC_nonfinite_state;
         if (a.codes && lane == 0) a.codes[sys] = code;
         store_stats<N, TS>(a, sys, st);
         if (a.cost && lane == 0) a.cost[sys] = st.c[ST_STEPS];
         TM::sync();
+    }
+}
+
+// ------------------------------------------------------------- factorisation only
+// E1 = (gamma/h) I - J and E2 = ((alpha + i beta)/h) I - J of one Jacobian per
+// block team, factored by the routine the Radau team kernels use at this
+// precision (Radau::decomp); the factors are copied out column-major (leading
+// dimension N) with perm[position] = original row and info[2] per matrix.
+template <class Mech, int TS, typename LT, typename L1>
+__global__ void __launch_bounds__(TS >= 32 ? TS : 32)
+decomp_kernel(int count, const double* jac, const double* h, L1* e1_out, cx<LT>* e2_out, int* perm_out,
+              int* info_out, TeamLayout lay)
+{
+    constexpr int N = Mech::N;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int m = blockIdx.x;
+    if (m >= count) return;
+    RadauTeamStore<N, LT, L1> store;
+    store.J = const_cast<double*>(jac) + size_t(m) * N * N;
+    store.E1 = reinterpret_cast<L1*>(smem + lay.e1);
+    store.E2 = reinterpret_cast<cx<LT>*>(smem + lay.e2);
+    store.d1 = reinterpret_cast<L1*>(smem + lay.d1);
+    store.d2 = reinterpret_cast<cx<LT>*>(smem + lay.d2);
+    store.p1 = reinterpret_cast<int*>(smem + lay.p1);
+    store.p2 = reinterpret_cast<int*>(smem + lay.p2);
+    store.buf = reinterpret_cast<double*>(smem + lay.buf);
+    store.rhs = reinterpret_cast<double*>(smem + lay.rhs);
+    store.inf = reinterpret_cast<int*>(smem + lay.inf);
+    Stats st;
+    st.clear();
+    Mech mech{};
+    Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>> rad{mech, store, RadauParams{1e-10, 1e-6}, 0.0, st};
+    rad.decomp(h[m]);
+    __syncthreads();
+    const int t = threadIdx.x;
+    for (int e = t; e < N * N; e += blockDim.x) {
+        e1_out[size_t(m) * N * N + e] = store.E1[e];
+        e2_out[size_t(m) * N * N + e] = store.E2[e];
+    }
+    for (int i = t; i < N; i += blockDim.x) {
+        perm_out[size_t(m) * 2 * N + i] = store.p1[i];
+        perm_out[size_t(m) * 2 * N + N + i] = store.p2[i];
+    }
+    __syncthreads();
+    if (t == 0) {
+        // Radau::decomp reports the first failing matrix; recompute both from the factors
+        int i1 = 0, i2 = 0;
+        for (int k = 0; k < N && (!i1 || !i2); ++k) {
+            if (!i1 && store.E1[k + k * N] == L1(0)) i1 = k + 1;
+            if (!i2 && store.E2[k + k * N].re == LT(0) && store.E2[k + k * N].im == LT(0)) i2 = k + 1;
+        }
+        info_out[2 * m] = i1;
+        info_out[2 * m + 1] = i2;
     }
 }
 

@@ -182,8 +182,8 @@ __device__ __forceinline__ void permute(Vec<N, TS>& x, const int* perm, double* 
 // pattern of RK_Solve (radau2a.c:404,417).  b arrives permuted; x stays
 // distributed in registers; column j of L/U is read by all lanes (coalesced).
 // Zero entries of the running solution skip their column as in dtrsm.
-template <int N, int TS, typename T>
-__device__ void lu_solve_pair(const T* A1, const T* d1, Vec<N, TS>& x1,
+template <int N, int TS, typename T1, typename T>
+__device__ void lu_solve_pair(const T1* A1, const T1* d1, Vec<N, TS>& x1,
                               const cx<T>* A2, const cx<T>* d2, Vec<N, TS>& x2r, Vec<N, TS>& x2i)
 {
     using TM = Team<TS>;

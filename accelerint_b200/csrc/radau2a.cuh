@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "linalg.cuh"
 #include "wlinalg.cuh"
+#include "rlinalg.cuh"
 #include "mlp.cuh"
 
 namespace aib {
@@ -73,19 +74,20 @@ constexpr double ELO = 4;
 
 // Matrix storage of one team: shared memory for teams of several lanes (J may
 // live in global scratch), registers/local memory for a thread per system.
-template <int N, typename LT> struct RadauRegStore {
-    using E1T = LT;
+// L1 is the precision of E1 (the matrix of the error estimate), LT that of E2.
+template <int N, typename LT, typename L1 = LT> struct RadauRegStore {
+    using E1T = L1;
     double J[N * N];
-    LT E1[N * N];
+    L1 E1[N * N];
     cx<LT> E2[N * N];
-    LT d1[N];
+    L1 d1[N];
     cx<LT> d2[N];
     int p1[N], p2[N];
     double buf[N];
     __device__ double* jac() { return J; }
-    __device__ LT* e1() { return E1; }
+    __device__ L1* e1() { return E1; }
     __device__ cx<LT>* e2() { return E2; }
-    __device__ LT* dinv1() { return d1; }
+    __device__ L1* dinv1() { return d1; }
     __device__ cx<LT>* dinv2() { return d2; }
     __device__ int* perm1() { return p1; }
     __device__ int* perm2() { return p2; }
@@ -197,6 +199,20 @@ struct Radau {
         L1* E1 = st.e1();
         cx<LT>* E2 = st.e2();
         const double g = radau::GAMMA / H, ar = radau::ALPHA / H, ai = radau::BETA / H;
+        if constexpr (Team<TS>::block && TS == 32 && N <= TS && sizeof(LT) == 4 && sizeof(L1) == 4) {
+            // single precision on a one-warp team: each matrix assembled and factored in
+            // registers (slu_factor, rlinalg.cuh), E2 first, then E1.  The matrices hold
+            // their multipliers while they are factored: E2's exchange slots go to E1's
+            // region (factored afterwards), E1's to the dydt scratch.
+            stats.c[ST_DECOMP]++;
+            const int i2 = slu_factor<N, TS, true>(J, ar, ai, reinterpret_cast<float*>(E2), st.perm2(),
+                                                   reinterpret_cast<float*>(st.dinv2()),
+                                                   reinterpret_cast<unsigned char*>(E1));
+            const int i1 = slu_factor<N, TS, false>(J, g, 0.0, reinterpret_cast<float*>(E1), st.perm1(),
+                                                    reinterpret_cast<float*>(st.dinv1()),
+                                                    reinterpret_cast<unsigned char*>(st.scratch_rhs()));
+            return i1 != 0 ? i1 : i2;
+        }
         const int lane = TM::lane();
         // block teams store lu_cols(N) columns, the ones past N zero (see wlinalg.cuh)
         constexpr int NC = Team<TS>::block ? lu_cols(N) : N;
@@ -208,7 +224,7 @@ struct Radau {
                 for (int j0 = 0; j0 < NC; j0 += 8) {
                     double v[8];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) v[c] = (j0 + c < N) ? -J[i + (j0 + c) * N] : 0.0;
+                    for (int c = 0; c < 8; ++c) v[c] = (j0 + c < N) ? -__ldcg(J + i + (j0 + c) * N) : 0.0;
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
                         const int j = j0 + c;
@@ -255,7 +271,7 @@ struct Radau {
             TM::sync();
             return info;
         } else {
-            int info = lu_real<N, TS, LT>(E1, st.perm1(), st.dinv1());
+            int info = lu_real<N, TS, L1>(E1, st.perm1(), st.dinv1());
             if (info != 0) return info;
             return lu_cplx<N, TS, LT>(E2, st.perm2(), st.dinv2());
         }
@@ -310,7 +326,7 @@ struct Radau {
             permute<N, TS>(R1, st.perm1(), buf);
             permute<N, TS>(R2, st.perm2(), buf);
             permute<N, TS>(R3, st.perm2(), buf);
-            lu_solve_pair<N, TS, LT>(st.e1(), st.dinv1(), R1, st.e2(), st.dinv2(), R2, R3);
+            lu_solve_pair<N, TS, L1, LT>(st.e1(), st.dinv1(), R1, st.e2(), st.dinv2(), R2, R3);
         }
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -341,7 +357,7 @@ struct Radau {
                 // four partial sums: the Jacobian loads are issued together
                 double a[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-                for (int j = 0; j < N; ++j) a[j & 3] = fma(J[t + N * j], buf[j], a[j & 3]);
+                for (int j = 0; j < N; ++j) a[j & 3] = fma(__ldcg(J + t + N * j), buf[j], a[j & 3]);
                 jx = (a[0] + a[1]) + (a[2] + a[3]);
             }
             V r;
@@ -351,7 +367,7 @@ struct Radau {
             x[0] += r[0];
             return;
         }
-        if (sizeof(LT) == sizeof(double)) {
+        if (sizeof(L1) == sizeof(double)) {
             permute<N, TS>(x, st.perm1(), buf);
             lu_solve_real<N, TS, L1>(st.e1(), st.dinv1(), x);
             return;

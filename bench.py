@@ -1,30 +1,43 @@
 #!/usr/bin/env python
 """Throughput benchmark: ODE systems/s per global Delta-t step.
 
-Workload (default): the 53-species / 325-reaction synthetic mechanism, 65,536
+Workload (default): the 53-species / 325-reaction synthetic mechanism, 1,048,576
 initial conditions of the mixed-stiffness generator (half near equilibrium at
 800-1200 K, half ignition at 1400-2400 K, interleaved), Radau IIA at rtol 1e-6 /
-atol 1e-10, global steps of dt = 1e-6 s from t = 0.  The 1,048,576-IC batch is
-`--num 1048576`; one global step of it takes minutes, so the default run uses a
-65,536-IC batch from the same generator.  A bench step is one global Delta-t
-step of all systems; the timed region runs K consecutive global steps starting
-from the initial conditions (the warm-up runs W steps from the same initial
-conditions, then the state is reset), so the transient after t = 0 is always
-inside the timed region.  L2 is flushed (a 256 MiB write) between timed steps,
-outside the per-step event pairs.
+atol 1e-10, global steps of dt = 1e-6 s from t = 0 (the reference's global-step
+loop, generic/solver_interface.cu:161-211).  A bench step is one global Delta-t
+step of all systems; the timed region runs K consecutive global steps from the
+initial conditions.  The W warm-up steps run the same calls on the whole batch
+with a global step of dt / 1000 (every buffer, graph and code path of the timed
+calls, about one Radau step per system), after which the state is reset.
+
+Timed region, one loop for both numbers: every step copies the state from
+pinned host memory to the device, integrates it through the C-ABI
+(accelerInt_integrate_device), and copies the state and the codes back; L2 is
+flushed (a 256 MiB write) before each step.  `value` is K x NUM over the summed
+CUDA-event time of the integrate calls (inputs resident), `e2e` is K x NUM over
+the wall time of the whole loop (copies included).
 
 The tuned form is three changes on top of the plain FP64 form:
 E1/E2 factorised and solved in FP32 (--lu), the persistent work-queue kernel
 under a captured CUDA graph with the autotuned mapping and a longest-first
 queue order from a learned per-system cost model (--queue-order 3), and the
 learned step-size proposals (--learned).  Both networks are trained, untimed,
-by the library's kernels on plain Radau runs of batches drawn with other seeds.  The plain FP64 form (one
-team per system over a plain grid, FP64 factorisations, no proposals) is timed
-on the same batch for `--plain-steps` global steps and reported as
-"plain_fp64" with the tuned / plain ratio.
+by the library's kernels on plain Radau runs of batches drawn with other seeds.
+The plain FP64 form (one team per system over a plain grid, FP64
+factorisations, no proposals) is timed on the same batch and steps and reported
+as "plain_fp64" with the tuned / plain ratio.
+
+Accuracy (untimed): the first --acc-sample systems (both stiffness halves) of
+the tuned and plain final states, and of the reference CPU radau2a at rtol 1e-6,
+against the oracle integrated at rtol 1e-12 / atol 1e-20 over the same global
+steps; the oracle runs in a separate process on the host cores while the GPU
+works.  Errors use the reference's weighted metric |x - x_ref| / (atol + rtol
+|x_ref|) with atol 1e-10, rtol 1e-6 (logger.py:53-55), and the maximum
+relative error of T and of the mass fractions above 1e-8.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--lu fp32|fp64] [--num NUM] [--solver radau2a]
+                    [--lu fp32|fp32_all|fp64] [--num NUM]
 
 For N > 1 (torchrun, one rank per GPU) every rank integrates its own batch of
 NUM systems (weak scaling, no collective on the data path); the time is the
@@ -60,10 +73,12 @@ def parse():
     p.add_argument("--lu", default="fp32_all", choices=["fp32", "fp32_all", "fp64"])
     p.add_argument("--plain-steps", type=int, default=-1,
                    help="global steps of the plain FP64 comparison (-1: as --steps, 0: skip)")
-    p.add_argument("--num", type=int, default=1 << 16)
+    p.add_argument("--num", type=int, default=1 << 20)
     p.add_argument("--solver", default="radau2a")
     p.add_argument("--seed", type=int, default=2024)
-    p.add_argument("--cpu-sample", type=int, default=0, help="systems in the CPU baseline sample (0: auto)")
+    p.add_argument("--cpu-sample", type=int, default=16384, help="systems in the CPU baseline sample")
+    p.add_argument("--acc-sample", type=int, default=1024,
+                   help="systems compared with the rtol-1e-12 oracle after the timed steps (0: none)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
@@ -100,20 +115,85 @@ def workload(num, seed, rank=0):
 
 
 # ---------------------------------------------------------------- FLOP model
-def flops_per_system(stats, n=54, R=325):
-    """Algorithmic FP64 flops from the device event counters (FMA = 2 flops).
+LU_NAMES = {"fp64": 0, "fp32": 1, "fp32_all": 2}
 
-    decomp: (2/3) N^3 real LU + (8/3) N^3 complex LU + N^2 (E1/E2 assembly);
-    newton: 3 RHS (counted separately) + 2 N^2 real + 8 N^2 complex triangular
-            solves + 30 N for transforms/updates + 12 N for the norms;
-    aux (error-estimate solves): 2 N^2 + 8 N;
-    rhs: 14 R + 10 N mass-action evaluation (2 exp counted as 0 flops);
-    jac: 60 R + 4 N^2."""
+
+def flops_per_system(stats, n=54, R=325, lu="fp64"):
+    """Algorithmic flops from the device event counters (FMA = 2 flops), split by the
+    pipe that runs them: returns (fp64 flops, fp32 flops) per system.
+
+    decomp:  (2/3) N^3 real LU (E1) + (8/3) N^3 complex LU (E2) + N^2 assembly (FP64);
+    newton:  3 RHS (counted separately) + 2 N^2 real (E1) + 8 N^2 complex (E2)
+             triangular solves + 42 N transforms, updates and norms (FP64);
+    aux:     one error-estimate solve with E1, 2 N^2, + 8 N (FP64); with E1 in FP32
+             (fp32_all) it is two FP32 solves (4 N^2) and the FP64 refinement
+             residual J x (2 N^2);
+    rhs:     14 R + 10 N mass-action evaluation (exponentials not counted);
+    jac:     60 R + 4 N^2.
+    The factorisations and solves of a matrix held in FP32 are FP32 flops (E2 for
+    lu fp32; E1 and E2 for fp32_all), everything else FP64."""
     d, nw, rhs, aux, jac = (stats[:, 4], stats[:, 5], stats[:, 6], stats[:, 7], stats[:, 3])
-    f = (d * ((2.0 / 3.0) * n ** 3 + (8.0 / 3.0) * n ** 3 + n * n) +
-         nw * (2 * n * n + 8 * n * n + 42 * n) + aux * (2 * n * n + 8 * n) +
-         rhs * (14 * R + 10 * n) + jac * (60 * R + 4 * n * n))
-    return f
+    lu1 = (2.0 / 3.0) * n ** 3
+    lu2 = (8.0 / 3.0) * n ** 3
+    fp64 = d * n * n + nw * 42 * n + rhs * (14 * R + 10 * n) + jac * (60 * R + 4 * n * n)
+    fp32 = np.zeros_like(fp64)
+    e1_32 = lu == "fp32_all"
+    e2_32 = lu in ("fp32", "fp32_all")
+    if e1_32:
+        fp32 = fp32 + d * lu1 + nw * 2 * n * n + aux * 4 * n * n
+        fp64 = fp64 + aux * (2 * n * n + 8 * n)
+    else:
+        fp64 = fp64 + d * lu1 + nw * 2 * n * n + aux * (2 * n * n + 8 * n)
+    if e2_32:
+        fp32 = fp32 + d * lu2 + nw * 8 * n * n
+    else:
+        fp64 = fp64 + d * lu2 + nw * 8 * n * n
+    return fp64, fp32
+
+
+def accuracy(y, y_tight, atol=1e-10, rtol=1e-6):
+    """Errors of final states y[N, m] against the tight oracle's: the reference's weighted
+    metric |x - x_ref| / (atol + rtol |x_ref|) (logger.py:53-55) per system (max over the
+    state), and the maximum relative errors of T (row 0) and of mass fractions above 1e-8."""
+    w = np.max(np.abs(y - y_tight) / (atol + rtol * np.abs(y_tight)), axis=0)
+    rel_t = np.abs(y[0] - y_tight[0]) / np.abs(y_tight[0])
+    big = np.abs(y_tight[1:]) > 1e-8
+    rel_y = np.where(big, np.abs(y[1:] - y_tight[1:]) / np.where(big, np.abs(y_tight[1:]), 1.0), 0.0)
+    finite = bool(np.isfinite(y).all())
+    return {"weighted_max": float(np.max(w)), "weighted_median": float(np.median(w)),
+            "frac_within_tol": float(np.mean(w < 1.0)), "rel_T_max": float(np.max(rel_t)),
+            "rel_Y_max": float(np.max(rel_y)), "finite": finite}
+
+
+def start_tight_oracle(y, var, t_end, nthreads, path):
+    """The rtol-1e-12 oracle over [0, t_end] in steps of DT, in a fresh process (oracle/tight.py)."""
+    import tempfile
+    fd, src = tempfile.mkstemp(prefix="accelerint_tight_", suffix=".npz")
+    os.close(fd)
+    np.savez(src, y=y, var=var, t0=0.0, t_end=t_end, dt=DT, atol=1e-20, rtol=1e-12, mech="ma54",
+             nthreads=nthreads)
+    proc = subprocess.Popen([sys.executable, "-m", "oracle.tight", src, path], cwd=ROOT,
+                            stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+    return proc, src
+
+
+def finish_tight_oracle(handle, path, timeout=1800.0):
+    proc, src = handle
+    try:
+        proc.wait(timeout=timeout)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        proc.wait()
+    try:
+        os.remove(src)
+    except OSError:
+        pass
+    if proc.returncode != 0 or not os.path.exists(path):
+        return None
+    d = np.load(path)
+    y = np.array(d["y"])
+    os.remove(path)
+    return y
 
 
 class ClockSampler:
@@ -168,26 +248,25 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def measure_fp64_peak(torch):
+def measure_peak(kind):
+    """FMA throughput of this device (TFLOP/s): kind 1 FP64, 0 FP32 scalar, 2 FP32x2 packed."""
     from accelerint_b200 import load_library
     lib = load_library()
     import ctypes
     out = ctypes.c_double(0.0)
     lib.accelerInt_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
-    rc = lib.accelerInt_measure_fma_peak(1, ctypes.byref(out))
+    rc = lib.accelerInt_measure_fma_peak(kind, ctypes.byref(out))
     return out.value if rc == 0 else None
 
 
 # ---------------------------------------------------------------- CPU baseline
 def cpu_baseline(args, mech, y, var):
-    """Reference CPU radau2a (oracle/_ref, the reference's own C sources) on a bounded sample."""
+    """Reference CPU radau2a (oracle/_ref, the reference's own C sources, OpenMP) on the
+    first --cpu-sample systems over the K global steps; returns (line, final states)."""
     sys.path.insert(0, ROOT)
     from oracle import Reference, reference_available, Oracle, oracle_available
     nthreads = os.cpu_count() or 1
-    # 128 systems per thread: the first three 53-species global steps cost ~0.08 s
-    # per system on one core, so the sample takes ~10 s whatever the core count, and
-    # holds enough of the few very stiff systems for a stable rate
-    sample = args.cpu_sample or min(args.num, 16384, 128 * nthreads)
+    sample = min(args.num, args.cpu_sample)
     ys, vs = y[:, :sample].copy(), var[:sample].copy()
     if reference_available("radau2a", 54):
         ref = Reference("radau2a", 54)
@@ -205,10 +284,12 @@ def cpu_baseline(args, mech, y, var):
             ys, codes, _ = o.integrate("radau2a", mech, ys, vs, k * DT, (k + 1) * DT, nthreads=nthreads)
         el = time.time() - t0
     else:
-        return None
-    return {"value": sample * args.steps / el, "unit": UNIT, "cores": nthreads, "kind": kind,
-            "sample": f"first {sample} systems (both stiffness halves) x {args.steps} global steps from t=0, "
-                      f"{nthreads} OpenMP threads, {el:.2f} s"}
+        return None, None
+    line = {"value": sample * args.steps / el, "unit": UNIT, "cores": nthreads, "kind": kind,
+            "sample": f"rate measured on the first {sample} of the {args.num} systems (both stiffness "
+                      f"halves) x {args.steps} global steps from t=0 on {nthreads} OpenMP threads "
+                      f"({el:.1f} s); a per-system-step rate, not a timing of the whole batch"}
+    return line, ys
 
 
 def run_reference_arm(args):
@@ -216,7 +297,7 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     mech, y, var = workload(args.num, args.seed)
-    cb = cpu_baseline(args, mech, y, var)
+    cb, _ = cpu_baseline(args, mech, y, var)
     if cb is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) and oracle missing"}))
         return 0
@@ -224,8 +305,11 @@ def run_reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.num / cb["value"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": "mass-action 53 species / 325 reactions, mixed stiffness, "
-                                                       f"{args.num} ICs, dt=1e-6 s, radau2a rtol 1e-6 atol 1e-10",
-                                            "solver": "radau2a (reference CPU, OpenMP)"},
+                                                       f"{args.num} ICs, global steps of dt=1e-6 s from t=0, "
+                                                       "radau2a rtol 1e-6 atol 1e-10",
+                                            "solver": "radau2a (reference CPU, OpenMP)",
+                                            "timing": "sampled rate: ms_per_step = the full batch at the rate "
+                                                      "measured on the sample (cpu_baseline.sample)"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -245,6 +329,21 @@ def run_ours(args):
     dev = torch.device("cuda", local if ws > 1 else 0)
     mech, y, var = workload(args.num, args.seed, rank)
     lu = {"fp32": A.LU_FP32, "fp32_all": A.LU_FP32_ALL, "fp64": A.LU_FP64}[args.lu]
+
+    # CPU work first, on rank 0: the reference CPU baseline alone on the host cores, then
+    # the tight oracle for the accuracy sample in a separate process during the GPU work
+    cb, y_ref_cpu, tight = None, None, None
+    tight_path = os.path.join(ROOT, f".bench_tight_{os.getpid()}.npz")
+    acc_n = min(args.acc_sample, args.num)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            cb, y_ref_cpu = cpu_baseline(args, mech, y, var)
+        if acc_n > 0:
+            from oracle import oracle_available
+            if oracle_available():
+                tight = start_tight_oracle(y[:, :acc_n].copy(), var[:acc_n].copy(), args.steps * DT,
+                                           max(1, (os.cpu_count() or 2) - 2), tight_path)
+
     model, learn_info = None, None
     if args.learned:
         # train on plain-Radau step records of a batch drawn with another seed (untimed)
@@ -279,12 +378,23 @@ def run_ours(args):
     yd = y0.clone()
     codes = torch.zeros(args.num, dtype=torch.int32, device=dev)
     stats = torch.zeros((args.num, A.NSTATS), dtype=torch.int32, device=dev)
+    # the state between steps lives in pinned host memory (the end-to-end chain)
+    y_host = torch.from_numpy(np.ascontiguousarray(y)).pin_memory()
+    codes_host = torch.zeros(args.num, dtype=torch.int32).pin_memory()
 
     def barrier():
         if ws > 1:
             import torch.distributed as dist
             dist.barrier()
         torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v):
+        if ws > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([v], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            return float(tt.item())
+        return v
 
     # mapping picked by the library's autotuner on a sample (a copy; untimed), then
     # every launch of the tuned form goes through a captured CUDA graph
@@ -300,14 +410,17 @@ def run_ours(args):
             mapping["queue_order"] = args.queue_order
     if not args.no_graph:
         integ.set_graph_launch(True)
-    # warm-up: W global steps from the initial conditions, then reset
+    # warm-up: W global steps of dt/1000 on the whole batch through the timed calls, then reset
+    dtw = DT * 1e-3
     with torch.cuda.stream(stream):
         for k in range(args.warmup):
-            integ.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, codes, None, stream)
-        yd.copy_(y0)
+            yd.copy_(y_host, non_blocking=True)
+            integ.integrate_device(k * dtw, (k + 1) * dtw, dtw, yd, vd, codes, None, stream)
+            y_host.copy_(yd, non_blocking=True)
+    stream.synchronize()
+    y_host.copy_(torch.from_numpy(np.ascontiguousarray(y)))
     if args.queue_order >= 0:
         # a fresh history: the first timed step knows nothing of the warm-up's step counts
-        torch.cuda.synchronize(dev)
         integ.set_queue_order(args.queue_order)
     barrier()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -315,59 +428,69 @@ def run_ours(args):
     launches0 = integ.kernel_launches()
     with ClockSampler(dev.index) as clk:
         barrier()
+        t0 = time.perf_counter()
         with torch.cuda.stream(stream):
             for k in range(args.steps):
                 flush.fill_(k & 0xff)
+                yd.copy_(y_host, non_blocking=True)
                 evs[k][0].record(stream)
                 integ.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, codes, stats, stream)
                 evs[k][1].record(stream)
+                y_host.copy_(yd, non_blocking=True)
+                codes_host.copy_(codes, non_blocking=True)
+        stream.synchronize()
+        wall = time.perf_counter() - t0
         barrier()
     launches = integ.kernel_launches() - launches0
-    ms = sum(a.elapsed_time(b) for a, b in evs)
-    t_max = ms
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    nfail = int((codes != 0).sum().item())
-    # a non-finite state with code 0 would make a step look cheap: count them
-    nonfinite = int((~torch.isfinite(yd)).any(dim=0).sum().item())
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = sum(step_ms)
+    t_max = max_over_ranks(ms)
+    wall_max = max_over_ranks(wall)
+    y_tuned = y_host.numpy()
+    codes_np = codes_host.numpy()
+    nfail = int((codes_np != 0).sum())
+    # a non-finite state would make a step look cheap: count them
+    nonfinite = int((~np.isfinite(y_tuned)).any(axis=0).sum())
     st = stats.cpu().numpy().astype(np.float64)
-    flops = float(flops_per_system(st).sum())
+    f64, f32 = flops_per_system(st, mech.n_state, mech.n_reactions, args.lu)
+    flops64, flops32 = float(f64.sum()), float(f32.sum())
     # work of the timed steps: a global step lasts about max(total work / teams, the
     # slowest system), so run-to-run changes of the slowest system move the number
     work = {"radau_steps": int(st[:, 0].sum()), "rejected": int(st[:, 2].sum()), "factorisations": int(st[:, 4].sum()),
             "newton_iterations": int(st[:, 5].sum()), "rhs": int(st[:, 6].sum()),
-            "max_steps_one_system": int(st[:, 0].max()), "flops": flops}
+            "max_steps_one_system": int(st[:, 0].max()), "flops_fp64": flops64, "flops_fp32": flops32}
     value = ws * args.num * args.steps / (t_max / 1000.0)
-    peak = measure_fp64_peak(torch) if rank == 0 else None
-    achieved = flops / (ms / 1000.0) / 1e12
-    # DRAM bytes per launch from one ncu capture of the tuned kernel (1,480 systems, one
-    # global step: 4.72 MB read + written), scaled by the systems of this launch
-    traffic = 4.72e6 / 1480 * args.num if args.lu != "fp64" else None
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                "traffic_unit": "bytes per launch (ncu capture scaled by systems)",
-                "algorithmic_bytes": args.num * (2 * mech.n_state + 1) * 8,
-                "note": "algorithmic FP64 flops from device event counters per system "
-                        "(decomp, Newton, RHS, error solves, Jacobians) over the kernel time; "
-                        "peak = FP64 FMA microbenchmark measured in this run"}
-    # e2e: the C-ABI host path (accelerInt_integrate_status) with host buffers, copies inside the timing
     e2e = None
     if not args.no_e2e:
-        t0 = time.time()
-        yh = y.copy()
-        for k in range(args.steps):
-            yh, c, rc = integ.integrate(k * DT, (k + 1) * DT, DT, yh, var)
-        el = time.time() - t0
-        nb = args.num * (mech.n_state + 1) * 8
-        e2e = {"value": ws * args.num * args.steps / el, "unit": UNIT,
-               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": args.num * mech.n_state * 8 + args.num * 4}
-    integ.close()
+        nb = args.num * (mech.n_state * 8)
+        e2e = {"value": ws * args.num * args.steps / wall_max, "unit": UNIT,
+               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb + args.num * 4,
+               "path": "pinned host state -> device, accelerInt_integrate_device, state and codes -> pinned "
+                       "host, every step; wall time of the loop (the L2 flush writes included)"}
+    roofline = None
+    if rank == 0:
+        p64, p32s, p32x2 = measure_peak(1), measure_peak(0), measure_peak(2)
+        p32 = max(p32s or 0.0, p32x2 or 0.0) or None
+        a64 = flops64 / (ms / 1000.0) / 1e12
+        a32 = flops32 / (ms / 1000.0) / 1e12
+        f64r = a64 / p64 if p64 else None
+        f32r = a32 / p32 if p32 else None
+        roofline = {"bound": "fp64+fp32 (CUDA-core FMA pipes; the kernel is issue- and latency-bound, HBM ~0)",
+                    "achieved": a64 + a32, "peak": None, "unit": "TFLOP/s",
+                    "frac": (f64r or 0.0) + (f32r or 0.0),
+                    "fp64": {"achieved": a64, "peak": p64, "frac": f64r},
+                    "fp32": {"achieved": a32, "peak": p32, "peak_scalar_ffma": p32s, "peak_packed_ffma2": p32x2,
+                             "frac": f32r},
+                    "traffic": None,
+                    "algorithmic_bytes": args.num * (2 * mech.n_state + 1) * 8,
+                    "note": "algorithmic flops from device event counters per system, split by pipe "
+                            "(factorisations and solves of the FP32 matrices on the FP32 pipe, the rest FP64), "
+                            "over the summed event time of the timed launches; peaks = FMA microbenchmarks "
+                            "measured in this run (FP32: the larger of scalar and packed FP32x2); frac = the sum "
+                            "of the two pipes' fractions"}
 
-    # the plain FP64 form on the same batch, for the tuned-vs-plain ratio
-    plain = None
+    # the plain FP64 form on the same batch and steps, for the tuned-vs-plain ratio
+    plain, y_plain = None, None
     if args.plain_steps > 0 and args.lu != "fp64":
         # the plain form: FP64 factorisations, one team per system over a plain grid
         # (no work queue, no graph, no tuning)
@@ -375,7 +498,7 @@ def run_ours(args):
         pinteg.set_persistent(False)
         nw = min(args.num, 4 * 148)
         yw = y0[:, :nw].contiguous()
-        pinteg.integrate_device(0.0, DT, DT, yw, vd[:nw].contiguous(), None, None, stream)   # warm-up
+        pinteg.integrate_device(0.0, dtw, dtw, yw, vd[:nw].contiguous(), None, None, stream)   # warm-up
         yd.copy_(y0)
         pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(args.plain_steps)]
@@ -387,19 +510,32 @@ def run_ours(args):
                 pinteg.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, None, None, stream)
                 pev[k][1].record(stream)
         barrier()
-        pms = sum(a.elapsed_time(b) for a, b in pev)
-        if ws > 1:
-            import torch.distributed as dist
-            tt = torch.tensor([pms], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            pms = float(tt.item())
+        pstep = [a.elapsed_time(b) for a, b in pev]
+        pms = max_over_ranks(sum(pstep))
         pinteg.close()
         pval = ws * args.num * args.plain_steps / (pms / 1000.0)
+        # tuned over the same global steps
+        tms = max_over_ranks(sum(step_ms[:args.plain_steps]))
+        tval = ws * args.num * args.plain_steps / (tms / 1000.0)
         plain = {"value": pval, "unit": UNIT, "ms_per_step": pms / args.plain_steps, "steps": args.plain_steps,
-                 "tuned_over_plain": value / pval}
+                 "tuned_over_plain": tval / pval, "ms_per_global_step": pstep}
+        if args.plain_steps == args.steps:
+            y_plain = yd[:, :acc_n].cpu().numpy()
+    integ.close()
 
     if rank == 0:
-        cb = None if args.no_cpu_baseline else cpu_baseline(args, mech, y, var)
+        acc = None
+        if tight is not None:
+            y_tight = finish_tight_oracle(tight, tight_path)
+            if y_tight is not None:
+                acc = {"oracle": "oracle radau2a at rtol 1e-12 / atol 1e-20 (plain-C restatement of "
+                                 "radau2a/radau2a.c)", "systems": acc_n,
+                       "interval": f"0 .. {args.steps} x 1e-6 s in global steps of 1e-6 s",
+                       "tuned": accuracy(y_tuned[:, :acc_n], y_tight)}
+                if y_plain is not None:
+                    acc["plain_fp64"] = accuracy(y_plain, y_tight)
+                if y_ref_cpu is not None and y_ref_cpu.shape[1] >= acc_n:
+                    acc["reference_cpu_rtol1e-6"] = accuracy(y_ref_cpu[:, :acc_n], y_tight)
         mb = args.num * mech.n_state * 8 / 1e6
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
@@ -411,12 +547,13 @@ def run_ours(args):
                                        f"atol 1e-10, LU {args.lu}, persistent work-queue team kernel"
                                        + (f", learned proposals {args.learned}" if args.learned else ""),
                            "l2": f"L2 flushed (256 MiB write) before every timed step; state y is {mb:.0f} MB",
+                           "warmup": f"{args.warmup} global steps of dt/1000 on the whole batch, then reset",
                            "failed_systems": nfail, "nonfinite_systems": nonfinite,
                            "mapping": mapping, "launch": "persistent kernel, "
                            + ("captured CUDA graph" if not args.no_graph else "direct launch")},
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain, "learned": learn_info,
-                "work": work}
+                "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain, "accuracy": acc,
+                "learned": learn_info, "work": work, "ms_per_global_step": step_ms}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist

@@ -16,7 +16,9 @@
  * Differences from the reference, by design:
  *   - no process exit on a failed system or CUDA error: the legacy void calls
  *     record the status (accelerInt_last_status) and per-system codes
- *     (accelerInt_get_codes, the reference's EC_* values 0..4);
+ *     (accelerInt_get_codes, the reference's EC_* values 0..4, plus
+ *     ACCELERINT_EC_NONFINITE where the reference would report success for a
+ *     system whose final state is not finite);
  *   - no cudaDeviceReset in initialize/cleanup (it destroys other users'
  *     contexts in the same process);
  *   - solver, mechanism, tolerances and precision are chosen at run time
@@ -60,6 +62,12 @@ void accelerInt_cleanup(void);
 #define ACCELERINT_ERR_STATE -3         /* not initialised / no mechanism */
 #define ACCELERINT_ERR_UNSUPPORTED -4   /* (solver, mechanism size, precision) not built */
 #define ACCELERINT_ERR_SYSTEMS -5       /* at least one system returned a nonzero EC_* code */
+
+/* Per-system code beyond the reference's EC_* values 0..4 (radau2a_props.h:288-296):
+ * the integrator finished without an error but the final state holds a NaN or an
+ * infinity.  The reference returns 0 for such a system (e.g. exp4, whose error norm
+ * accepts a NaN estimate); here it is reported. */
+#define ACCELERINT_EC_NONFINITE 5
 
 /* solvers (generic/solver_props.h:9-16 selects one of these at compile time) */
 #define ACCELERINT_RADAU2A 0
@@ -124,11 +132,16 @@ int accelerInt_integrate_device(int NUM, double t_start, double t_end, double st
  * Limits: mass-action mechanism and Radau only; the number of systems in flight
  * is capped by what fits in 16 MiB (719 at N = 54, so it can be slower than
  * accelerInt_integrate_device); a state length whose single N x N Jacobian does
- * not fit is rejected with ACCELERINT_ERR_ARGUMENT.  The first call on a device
- * looks up the array's device address; make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
- * streams, other threads) race and must be serialised by the caller.
- * accelerInt_initialize and the mechanism setters must have run before. */
+ * not fit is rejected with ACCELERINT_ERR_ARGUMENT.  The Jacobian mode and LU
+ * precision are honoured as accelerInt_integrate_device honours them (finite
+ * differences: plain FP64 only); with learned proposals or step recording
+ * installed the call returns ACCELERINT_ERR_UNSUPPORTED.  The first call on a
+ * device looks up the array's device address; make that first call before any
+ * stream capture.  accelerInt_initialize and accelerInt_cleanup drop the looked-up
+ * addresses, so the next call looks them up again.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  accelerInt_initialize and the mechanism setters must
+ * have run before. */
 int accelerInt_integrate_device_noalloc(int NUM, double t_start, double t_end, double stepsize,
                                         double* y_dev, const double* var_dev, int* codes_dev, void* stream);
 
@@ -212,13 +225,28 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
                         const double* var_dev, int sample, int* occupancy_cap_out, int* tps_block_out,
                         double* best_ms_out);
 
+/* Diagnostic: the factorisations of the Radau simplified-Newton matrices alone.
+ * For each of `count` Jacobians jac_dev[m * n * n + i + j * n] (column-major) and
+ * step sizes h_dev[m], factors E1 = (gamma/h) I - J and E2 = ((alpha + i beta)/h) I - J
+ * with the routine the Radau kernels use at `precision` (RK_Decomp,
+ * radau2a/radau2a.c:256-278: partial-pivot LU with xGETF2 semantics) and writes
+ * the factors column-major: e1_dev[m * n * n + ...] (double, or float for
+ * ACCELERINT_LU_FP32_ALL), e2_dev (interleaved complex: double pairs for
+ * ACCELERINT_LU_FP64, float pairs otherwise), perm_dev[m * 2n + position] = original
+ * row (E1 then E2) and info_dev[2m], info_dev[2m + 1] (k + 1 at the first zero
+ * pivot, else 0).  State lengths n = 14 and 54.  Device pointers; asynchronous. */
+int accelerInt_radau_decomp(int n, int precision, int count, const double* jac_dev, const double* h_dev,
+                            void* e1_dev, void* e2_dev, int* perm_dev, int* info_dev, void* stream);
+
 /* Extension: number of kernels this library has launched in the process. */
 long long accelerInt_kernel_launches(void);
 const char* accelerInt_version(void);
 
 /* Diagnostic: measured FMA throughput of the current device in TFLOP/s (FMA = 2
- * flops), fp64 != 0 for double precision, else single.  Used as the roofline
- * denominator for the FP64/FP32 integrator kernels. */
+ * flops): fp64 = 1 double precision, 0 single precision (scalar FFMA), 2 single
+ * precision as packed FP32x2 FMAs (two FMAs per instruction, the form the
+ * single-precision factorisations use).  The roofline denominators of the
+ * integrator kernels. */
 int accelerInt_measure_fma_peak(int fp64, double* tflops);
 
 #ifdef __cplusplus

@@ -32,9 +32,31 @@ def test_flop_model_counts_events():
     import bench
     st = np.zeros((2, 10))
     st[0, 4] = 1          # one factorisation at N = 54
-    f = bench.flops_per_system(st)
-    assert f[1] == 0.0
-    assert abs(f[0] - ((2.0 / 3.0 + 8.0 / 3.0) * 54 ** 3 + 54 * 54)) < 1e-6
+    lu1, lu2 = (2.0 / 3.0) * 54 ** 3, (8.0 / 3.0) * 54 ** 3
+    f64, f32 = bench.flops_per_system(st)
+    assert f64[1] == 0.0 and f32[1] == 0.0
+    assert abs(f64[0] - (lu1 + lu2 + 54 * 54)) < 1e-6 and f32[0] == 0.0
+    # the factorisations of FP32 matrices are FP32 flops: E2 for fp32, both for fp32_all
+    f64, f32 = bench.flops_per_system(st, lu="fp32")
+    assert abs(f64[0] - (lu1 + 54 * 54)) < 1e-6 and abs(f32[0] - lu2) < 1e-6
+    f64, f32 = bench.flops_per_system(st, lu="fp32_all")
+    assert abs(f64[0] - 54 * 54) < 1e-6 and abs(f32[0] - (lu1 + lu2)) < 1e-6
+    # a Newton iteration: the triangular solves follow the matrices' precision
+    st[0, 4], st[0, 5] = 0, 1
+    f64, f32 = bench.flops_per_system(st, lu="fp32_all")
+    assert abs(f32[0] - 10 * 54 * 54) < 1e-6 and abs(f64[0] - 42 * 54) < 1e-6
+
+
+def test_accuracy_metrics():
+    sys.path.insert(0, ROOT)
+    import bench
+    ref = np.array([[1000.0, 2000.0], [0.5, 1e-12], [0.5, 1.0]])
+    y = ref.copy()
+    y[0, 1] *= 1 + 2e-6
+    a = bench.accuracy(y, ref)
+    assert abs(a["rel_T_max"] - 2e-6) < 1e-12
+    assert a["rel_Y_max"] == 0.0 and a["finite"]
+    assert abs(a["weighted_max"] - 4e-3 / (1e-10 + 2e-3)) < 1e-6 and a["frac_within_tol"] == 0.5
 
 
 def test_state_features_layout():
