@@ -28,9 +28,6 @@ int predict_cost(const float* params, const float* norm, int num, int n, const d
 namespace {
 
 // FMA throughput probe: 8 independent dependency chains per thread.
-__device__ __forceinline__ float2 fma_probe(float2 a, float2 m, float2 c) { return __ffma2_rn(a, m, c); }
-__device__ __forceinline__ float fma_probe(float a, float m, float c) { return fmaf(a, m, c); }
-__device__ __forceinline__ double fma_probe(double a, double m, double c) { return fma(a, m, c); }
 __global__ void fma_peak_kernel2(float2* out, int iters, float2 m) {
     float2 a[8];
 #pragma unroll
@@ -38,7 +35,7 @@ __global__ void fma_peak_kernel2(float2* out, int iters, float2 m) {
     const float2 d = make_float2(1e-7f, 1e-7f);
     for (int i = 0; i < iters; ++i) {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) a[c] = fma_probe(a[c], m, d);
+        for (int c = 0; c < 8; ++c) a[c] = __ffma2_rn(a[c], m, d);
     }
     float2 s = make_float2(0.f, 0.f);
 #pragma unroll

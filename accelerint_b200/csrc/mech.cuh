@@ -259,7 +259,11 @@ __device__ __noinline__ void ma_jacob(double P, double yi, double* J, double* sm
         hgp = h[k] * g;
         Qp = h[k] * w;
         dQTp = __ldg(tb.cp + k) * w + h[k] * wT;
-        // dense part of row t, then the sparse G entries of the same row
+        // dense part of row t, then the sparse G entries of the same row.  The
+        // sparse additions are reductions without a returned value: the thread
+        // does not wait for the scattered read-modify-writes (they are ordered
+        // after its own stores to the same entries, and the barrier at the end
+        // makes them visible to the team)
         const double a = w * inv_c0 - g;
         const double wmk = __ldg(tb.mw + k);
         for (int j = 0; j < K; ++j) J[t + N * (1 + j)] = wmk * __ldg(tb.inv_mw + j) * a;
@@ -269,10 +273,10 @@ __device__ __noinline__ void ma_jacob(double P, double yi, double* J, double* sm
             const int r = ent >> 2;
             const double nu = (ent & 3) < 2 ? -1.0 : 1.0;
             const int4 sp = __ldg(tb.rsp + r);
-            J[t + N * (1 + sp.x)] += wmk * __ldg(tb.inv_mw + sp.x) * nu * dqC[4 * r + 0];
-            if (sp.y >= 0) J[t + N * (1 + sp.y)] += wmk * __ldg(tb.inv_mw + sp.y) * nu * dqC[4 * r + 1];
-            J[t + N * (1 + sp.z)] += wmk * __ldg(tb.inv_mw + sp.z) * nu * dqC[4 * r + 2];
-            if (sp.w >= 0) J[t + N * (1 + sp.w)] += wmk * __ldg(tb.inv_mw + sp.w) * nu * dqC[4 * r + 3];
+            atomicAdd(J + t + N * (1 + sp.x), wmk * __ldg(tb.inv_mw + sp.x) * nu * dqC[4 * r + 0]);
+            if (sp.y >= 0) atomicAdd(J + t + N * (1 + sp.y), wmk * __ldg(tb.inv_mw + sp.y) * nu * dqC[4 * r + 1]);
+            atomicAdd(J + t + N * (1 + sp.z), wmk * __ldg(tb.inv_mw + sp.z) * nu * dqC[4 * r + 2]);
+            if (sp.w >= 0) atomicAdd(J + t + N * (1 + sp.w), wmk * __ldg(tb.inv_mw + sp.w) * nu * dqC[4 * r + 3]);
         }
     }
     const double hg = TM::sum(hgp);

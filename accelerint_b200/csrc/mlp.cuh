@@ -59,9 +59,10 @@ __device__ __forceinline__ double symexp(double v) { return v >= 0 ? expm1(v) : 
 // One inference for the calling team.  x (D0 floats, raw features, entries past
 // N + 2 zero) and the two ping-pong buffers (MLP_D4 floats each) live in shared
 // memory; the raw (de-standardised) outputs end in `out` (one of the buffers,
-// returned).  Every thread of the team must call.
+// returned).  only >= 0: the last layer computes that output alone (the step-size
+// proposal needs one of its MLP_D4 rows).  Every thread of the team must call.
 template <int TS>
-__device__ __noinline__ float* mlp_infer_team(const MlpDevice& m, float* x, float* b0, float* b1)
+__device__ __noinline__ float* mlp_infer_team(const MlpDevice& m, float* x, float* b0, float* b1, int only = -1)
 {
     using TM = Team<TS>;
     const int lane = TM::lane();
@@ -73,7 +74,8 @@ __device__ __noinline__ float* mlp_infer_team(const MlpDevice& m, float* x, floa
         const int din = mlp_din(l), dout = mlp_dout(l);
         const __nv_bfloat16* W = m.w + mlp_wq(l);
         const float* b = m.p + mlp_boff(l);
-        for (int j = lane; j < dout; j += TS) {
+        const bool last = l == MLP_LAYERS - 1;
+        for (int j = (last && only >= 0) ? only + lane : lane; j < ((last && only >= 0) ? only + 1 : dout); j += TS) {
             const uint4* row = reinterpret_cast<const uint4*>(W + size_t(j) * din);
             float acc = b[j];
             for (int k8 = 0; k8 < din / 8; ++k8) {
@@ -92,7 +94,8 @@ __device__ __noinline__ float* mlp_infer_team(const MlpDevice& m, float* x, floa
         in = out;
     }
     float* y = ((MLP_LAYERS - 1) & 1) ? b1 : b0;
-    for (int j = lane; j < MLP_D4; j += TS) y[j] = y[j] * m.norm[2 * MLP_D0 + MLP_D4 + j] + m.norm[2 * MLP_D0 + j];
+    for (int j = only >= 0 ? only + lane : lane; j < (only >= 0 ? only + 1 : MLP_D4); j += TS)
+        y[j] = y[j] * m.norm[2 * MLP_D0 + MLP_D4 + j] + m.norm[2 * MLP_D0 + j];
     TM::sync();
     return y;
 }

@@ -463,7 +463,9 @@ struct Radau {
                     float* xb = reinterpret_cast<float*>(st.scratch_rhs());
                     mlp_features(y, Hprev, xb);
                     TM::sync();
-                    const float* o = mlp_infer_team<TS>(learn->mlp, xb, xb + MLP_D0, xb + MLP_D0 + MLP_D4);
+                    // without stage proposals only the step-size output is needed
+                    const float* o = mlp_infer_team<TS>(learn->mlp, xb, xb + MLP_D0, xb + MLP_D0 + MLP_D4,
+                                                        (mlp_flags & MLP_USE_Z) ? -1 : 3 * N);
                     const double Hp = Hprev * exp10(double(o[3 * N]));
                     if constexpr (LEARN >= 2) {
                       if (mlp_flags & MLP_USE_Z) {

@@ -31,7 +31,8 @@ class _Mech(ctypes.Structure):
 class _Config(ctypes.Structure):
     _fields_ = [("atol", ctypes.c_double), ("rtol", ctypes.c_double),
                 ("poles_re", ctypes.c_double * NRA), ("poles_im", ctypes.c_double * NRA),
-                ("res_re", ctypes.c_double * NRA), ("res_im", ctypes.c_double * NRA)]
+                ("res_re", ctypes.c_double * NRA), ("res_im", ctypes.c_double * NRA),
+                ("max_steps", ctypes.c_int)]
 
 
 _POLES = None
@@ -113,9 +114,10 @@ class Oracle:
         self.lib.or_complex_inverse_hessenberg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _ip]
         self.lib.or_complex_inverse_hessenberg.restype = ctypes.c_int
 
-    def config(self, atol=1e-10, rtol=1e-6, poles=None):
+    def config(self, atol=1e-10, rtol=1e-6, poles=None, max_steps=0):
         c = _Config()
         c.atol, c.rtol = atol, rtol
+        c.max_steps = max_steps
         p, r = poles if poles is not None else cf_poles(1e-10)
         for i in range(NRA):
             c.poles_re[i], c.poles_im[i] = p[i].real, p[i].imag
@@ -123,11 +125,12 @@ class Oracle:
         return c
 
     def integrate(self, solver, mech, y, var, t0, t1, atol=1e-10, rtol=1e-6, nthreads=0, poles=None,
-                  fd_jacobian=False):
-        """One global step [t0, t1] for every system.  Returns (y_new, codes, stats[num, NSTATS])."""
+                  fd_jacobian=False, max_steps=0):
+        """One global step [t0, t1] for every system.  Returns (y_new, codes, stats[num, NSTATS]).
+        max_steps: Radau step limit (0: the reference's 200000)."""
         keep = []
         m = _mech_struct(mech, keep, (atol, rtol) if fd_jacobian else None)
-        c = self.config(atol, rtol, poles)
+        c = self.config(atol, rtol, poles, max_steps)
         y = np.array(y, dtype=np.float64, order="C", copy=True)
         num = y.shape[1]
         var = np.ascontiguousarray(var, dtype=np.float64)

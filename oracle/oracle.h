@@ -49,6 +49,10 @@ typedef struct {
     double atol, rtol;
     /* rational-approximant poles and residues (exp methods) */
     double poles_re[OR_NRA], poles_im[OR_NRA], res_re[OR_NRA], res_im[OR_NRA];
+    /* Radau step limit per integrate call; 0: the reference's MAX_NO_STEPS (200000).
+     * A tight-tolerance oracle run raises it: at rtol 1e-12 a few ignition systems
+     * take more steps than the reference allows at its own tolerance. */
+    int max_steps;
 } or_config;
 
 /* Per-system counters; one row of OR_NSTATS doubles per system. */

@@ -250,7 +250,7 @@ int or_radau2a(const or_config* c, const or_mech* m, double t_start, double t_en
         }
         Nsteps += 1;
         st[ST_STEPS] += 1;
-        if (Nsteps >= MAX_NO_STEPS) return 2;                        /* EC_max_steps_exceeded */
+        if (Nsteps >= (c->max_steps > 0 ? c->max_steps : MAX_NO_STEPS)) return 2;   /* EC_max_steps_exceeded */
         if (0.1 * fabs(H) <= fabs(t) * ROUNDOFF) return 3;           /* EC_h_plus_t_equals_h */
         if (FirstStep) {
             memset(Z1, 0, n * sizeof(double));
