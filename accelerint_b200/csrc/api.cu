@@ -167,8 +167,29 @@ int upload_poles() {
     return ACCELERINT_OK;
 }
 
+// Species count of the kernels that serve a mechanism of K species: K itself for the
+// instantiated sizes (13, 53), else the next padded size (K + 1 rounded up to 16, 32,
+// 48 or 64 state elements).  Padding species have no reactions, unit molar mass and
+// zero heat capacity and enthalpy: their mass fractions stay zero and their rows and
+// columns leave the real ones unchanged (only the error norms need the real length).
+int device_species(int K) {
+    if (K == 13 || K == 53) return K;
+    const int n = K + 1;
+    return n <= 16 ? 15 : n <= 32 ? 31 : n <= 48 ? 47 : 63;
+}
+
 int upload_mass_action() {
-    const MechTablesHost& m = g.mt;
+    MechTablesHost m = g.mt;
+    const int kd = device_species(m.K);
+    for (int k = m.K; k < kd; ++k) {
+        m.mw.push_back(1.0);
+        m.inv_mw.push_back(1.0);
+        m.cp.push_back(0.0);
+        m.h_form.push_back(0.0);
+        m.s_ref.push_back(0.0);
+        m.sp_ptr.push_back(m.sp_ptr.back());
+    }
+    m.K = kd;
     if (g.dev_tb_mem) cudaFree(g.dev_tb_mem);
     g.dev_tb_mem = nullptr;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
@@ -310,6 +331,29 @@ int launch_krylov(BatchArgs a, const Mech& mech, int rhs_doubles, int jac_double
     return launch_team<SK_EXP4, Mech, TS, double>(a, mech, lay, s);
 }
 
+// Radau IIA on a mechanism padded to KP species (device_species): analytic
+// Jacobian, no learned proposals; the caller's state has n_state = K + 1 rows.
+template <int KP, int TS>
+int launch_mass_action_padded(BatchArgs a, cudaStream_t s) {
+    using M = MassAction<KP>;
+    M mech;
+    const int R = g.mt.R;
+    constexpr int N = M::N;
+    if (g.solver != ACCELERINT_RADAU2A || g.jac_mode != 0 || a.learn.mlp.flags || a.learn.rec)
+        return ACCELERINT_ERR_UNSUPPORTED;
+    a.n_state = g.mt.K + 1;
+    if (g.lu == ACCELERINT_LU_FP32) {
+        TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 8);
+        return launch_team<SK_RADAU, M, TS, float, double>(a, mech, lay, s);
+    }
+    if (g.lu == ACCELERINT_LU_FP32_ALL) {
+        TeamLayout lay = TeamLayout::radau(N, 4, M::smem_rhs(R), M::smem_jac(R), 4);
+        return launch_team<SK_RADAU, M, TS, float, float>(a, mech, lay, s);
+    }
+    TeamLayout lay = TeamLayout::radau(N, 8, M::smem_rhs(R), M::smem_jac(R));
+    return launch_team<SK_RADAU, M, TS, double>(a, mech, lay, s);
+}
+
 template <int K, int TS>
 int launch_mass_action(BatchArgs a, cudaStream_t s) {
     using M = MassAction<K>;
@@ -411,9 +455,13 @@ int launch_decomp_prec(int precision, int count, const double* jac, const double
 int launch(BatchArgs a, cudaStream_t s) {
     if (a.num <= 0) return ACCELERINT_OK;
     if (g.mech_kind == 0) return launch_vdp(a, s);
-    switch (g.mt.K) {
+    switch (device_species(g.mt.K)) {
         case 13: return launch_mass_action<13, 32>(a, s);
         case 53: return launch_mass_action<53, 64>(a, s);
+        case 15: return launch_mass_action_padded<15, 32>(a, s);
+        case 31: return launch_mass_action_padded<31, 32>(a, s);
+        case 47: return launch_mass_action_padded<47, 64>(a, s);
+        case 63: return launch_mass_action_padded<63, 64>(a, s);
         default: return ACCELERINT_ERR_UNSUPPORTED;
     }
 }

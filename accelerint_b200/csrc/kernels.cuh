@@ -37,6 +37,7 @@ struct BatchArgs {
     int plain_grid;         // team kernels: one team per system over a full grid, no work queue
     const int* order;       // queue order (system index of each queue slot), or null: index order
     int* cost;              // per-system steps of this call (written), or null
+    int n_state;            // the caller's state length (rows of y), when the kernel's N pads it; 0: N
 };
 
 // The reference's global-step loop (generic/solver_main.c:196-209), measured from t_start.
@@ -186,10 +187,12 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             sys = TM::bcast(sys, 0);
         }
         if (sys >= a.num) break;
+        // a padded mechanism (n_state < N) holds zeros in the rows past the caller's state
+        const int nst = a.n_state > 0 ? a.n_state : N;
         Vec<N, TS> y;
 #pragma unroll
         for (int s = 0; s < Vec<N, TS>::S; ++s)
-            y[s] = Vec<N, TS>::ok(s) ? a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] : 0.0;
+            y[s] = (Vec<N, TS>::ok(s) && Vec<N, TS>::idx(s) < nst) ? a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] : 0.0;
         const double pr = a.var[sys];
         Stats st;
         st.clear();
@@ -209,7 +212,7 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             store.inf = reinterpret_cast<int*>(base + lay.inf);
             const LearnArgs la = a.learn;
             Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>, LEARN> rad{mech, store,
-                                                                         RadauParams{a.atol, a.rtol},
+                                                                         RadauParams{a.atol, a.rtol, nst},
                                                                          pr, st, LEARN ? &la : nullptr};
             while (L.more() && code == EC_success) {
                 code = rad.integrate(L.t, L.t_next, y);
@@ -244,7 +247,7 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
         double bad = 0.0;
 #pragma unroll
         for (int s = 0; s < Vec<N, TS>::S; ++s)
-            if (Vec<N, TS>::ok(s)) {
+            if (Vec<N, TS>::ok(s) && Vec<N, TS>::idx(s) < nst) {
                 a.y[size_t(Vec<N, TS>::idx(s)) * a.num + sys] = y[s];
                 if (!isfinite(y[s])) bad = 1.0;
             }

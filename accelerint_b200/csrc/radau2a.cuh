@@ -129,6 +129,10 @@ template <int N, typename LT, typename L1 = LT> struct RadauTeamStore {
 
 struct RadauParams {
     double atol, rtol;
+    // state length of the error norms (radau2a.c:446-453 divide by NSP): N, or the
+    // caller's state length when the mechanism is padded to the next instantiated size
+    // (the padding rows stay zero and add nothing to the sums)
+    int n_eff = 0;
 };
 
 // LEARN (block teams only): 0 off; 1 step-size proposals and step records; 2 also
@@ -190,7 +194,7 @@ struct Radau {
         for (int s = 0; s < S; ++s)
             if (V::ok(s)) sum += sc[s] * sc[s] * d[s] * d[s];
         sum = TM::sum(sum);
-        return fmax(sqrt(sum / double(N)), 1e-10);
+        return fmax(sqrt(sum / double(prm.n_eff > 0 ? prm.n_eff : N)), 1e-10);
     }
 
     // radau2a.c:256-278; returns info (0 on success)

@@ -10,7 +10,8 @@ Two CPU implementations live here:
     length, per-system return codes and event counters;
   * oracle/_ref: the reference's own unmodified CPU sources compiled per
     (solver, state length), used to pin the restatement and as the timed
-    reference CPU baseline.
+    reference CPU baseline; and its GPU Radau (radau2a.cu under intDriver)
+    compiled for sm_100a, timed beside the library's kernels.
 """
-from .api import (SOLVERS, STAT_NAMES, Oracle, Reference, cf_poles, global_steps,  # noqa: F401
-                  oracle_available, reference_available)
+from .api import (SOLVERS, STAT_NAMES, Oracle, Reference, ReferenceGPU, cf_poles, global_steps,  # noqa: F401
+                  oracle_available, reference_available, reference_gpu_available)

@@ -262,3 +262,51 @@ class Reference:
             y, c = self.integrate(y, var, a, b, nthreads)
             codes = c if codes is None else np.maximum(codes, c)
         return y, codes
+
+
+def reference_gpu_available(n: int) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libref_gpu_radau2a_n{n}.so"))
+
+
+class ReferenceGPU:
+    """The reference's own GPU Radau IIA (radau2a/radau2a.cu under generic/solver_generic.cu's
+    intDriver, one thread per system), compiled unmodified by oracle/build.py with the
+    mechanism callbacks for state length n (2: the reference's van der Pol example; 54: the
+    synthetic mass-action mechanism, oracle/refshim/ma_gpu) and the host entry
+    oracle/refshim/ref_gpu_entry.cu.  Needs a GPU."""
+
+    def __init__(self, n: int):
+        self.n = n
+        self.lib = ctypes.CDLL(os.path.join(HERE, "_ref", f"libref_gpu_radau2a_n{n}.so"))
+        self.lib.refgpu_run.restype = ctypes.c_int
+        self.lib.refgpu_run.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp,
+                                        _ip, _dp]
+        self._keep = []
+
+    def set_mechanism(self, mech):
+        if self.n == 2:
+            return
+        arrs = [np.ascontiguousarray(getattr(mech, k), dtype=np.float64) for k in ("mw", "cp", "h_form", "s_ref")]
+        ints = [np.ascontiguousarray(getattr(mech, k), dtype=np.int32).reshape(-1) for k in ("reac", "prod")]
+        rates = [np.ascontiguousarray(getattr(mech, k), dtype=np.float64) for k in ("log_a", "beta", "ta")]
+        self._keep = arrs + ints + rates
+        f = self.lib.refgpu_set_mass_action
+        f.restype = ctypes.c_int
+        f.argtypes = [ctypes.c_int, ctypes.c_int] + [_dp] * 4 + [_ip] * 2 + [_dp] * 3
+        rc = f(mech.n_species, mech.n_reactions, *[a.ctypes.data_as(_dp) for a in arrs],
+               *[a.ctypes.data_as(_ip) for a in ints], *[a.ctypes.data_as(_dp) for a in rates])
+        if rc != 0:
+            raise RuntimeError(f"refgpu_set_mass_action failed ({rc})")
+
+    def run(self, y, var, t0, t_end, dt):
+        """Global steps t0 -> t_end of dt; returns (y_out, codes (max over steps), summed kernel ms)."""
+        y = np.array(y, dtype=np.float64, order="C", copy=True)
+        num = y.shape[1]
+        var = np.ascontiguousarray(var, dtype=np.float64)
+        codes = np.zeros(num, dtype=np.int32)
+        ms = ctypes.c_double(0.0)
+        rc = self.lib.refgpu_run(num, t0, t_end, dt, y.ctypes.data_as(_dp), var.ctypes.data_as(_dp),
+                                 codes.ctypes.data_as(_ip), ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"refgpu_run failed ({rc})")
+        return y, codes, ms.value
