@@ -86,13 +86,15 @@ struct Krylov {
         sync();
     }
 
-    // sparse_multiplier: w_i = sum_k J[i + N k] v_k, v in shared memory
+    // sparse_multiplier: w_i = sum_k J[i + N k] v_k, v in shared memory.  The Jacobian
+    // is read from L2 (ld.global.cg): a mechanism may write its entries with reductions,
+    // which the L1 copy of an earlier read would not see.
     __device__ __forceinline__ double jacvec_smem(const double* v) const {
         if (!own()) return 0.0;
         const int i = lane();
-        double acc = s.J[i] * v[0];
+        double acc = __ldcg(s.J + i) * v[0];
 #pragma unroll 6
-        for (int k = 1; k < N; ++k) acc += s.J[i + N * k] * v[k];
+        for (int k = 1; k < N; ++k) acc += __ldcg(s.J + i + N * k) * v[k];
         return acc;
     }
     __device__ __forceinline__ double jacvec(double vi) {

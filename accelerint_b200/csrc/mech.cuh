@@ -262,8 +262,9 @@ __device__ __noinline__ void ma_jacob(double P, double yi, double* J, double* sm
         // dense part of row t, then the sparse G entries of the same row.  The
         // sparse additions are reductions without a returned value: the thread
         // does not wait for the scattered read-modify-writes (they are ordered
-        // after its own stores to the same entries, and the barrier at the end
-        // makes them visible to the team)
+        // after its own stores to the same entries).  They are performed in L2,
+        // so every reader of the Jacobian loads it with ld.global.cg (__ldcg):
+        // an L1 line kept from an earlier read would miss them.
         const double a = w * inv_c0 - g;
         const double wmk = __ldg(tb.mw + k);
         for (int j = 0; j < K; ++j) J[t + N * (1 + j)] = wmk * __ldg(tb.inv_mw + j) * a;
@@ -301,7 +302,8 @@ __device__ __noinline__ void ma_jacob(double P, double yi, double* J, double* sm
     TM::sync();
 }
 
-// Mechanism object used by the integrators: block teams, one element per thread.
+// Mechanism object used by the integrators: teams of TS >= N lanes (a block, a warp
+// or part of a warp), one element per lane.
 template <int KS>
 struct MassAction {
     static constexpr int K = KS;
@@ -313,12 +315,12 @@ struct MassAction {
 
     template <int TS>
     __device__ __forceinline__ void dydt(double, double P, const Vec<N, TS>& y, Vec<N, TS>& dy, double* sm) const {
-        static_assert(Team<TS>::block && Vec<N, TS>::S == 1, "mass action runs on block teams, one element per thread");
+        static_assert(Vec<N, TS>::S == 1, "mass action runs on teams of at least N lanes, one element per lane");
         dy[0] = ma_dydt<K, TS>(P, y[0], sm);
     }
     template <int TS>
     __device__ __forceinline__ void jacob(double, double P, const Vec<N, TS>& y, double* J, double* sm) const {
-        static_assert(Team<TS>::block && Vec<N, TS>::S == 1, "mass action runs on block teams, one element per thread");
+        static_assert(Vec<N, TS>::S == 1, "mass action runs on teams of at least N lanes, one element per lane");
         ma_jacob<K, TS>(P, y[0], J, sm);
     }
 };

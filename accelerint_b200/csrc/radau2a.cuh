@@ -240,7 +240,7 @@ struct Radau {
         } else {
             for (int e = lane; e < N * NC; e += TS) {
                 const int i = e % N, j = e / N;
-                const double mj = j < N ? -J[e] : 0.0;
+                const double mj = j < N ? -__ldcg(J + e) : 0.0;
                 E1[e] = L1(i == j ? mj + g : mj);
                 E2[e] = cx<LT>{LT(i == j ? mj + ar : mj), LT(i == j ? ai : 0.0)};
             }
@@ -393,7 +393,7 @@ struct Radau {
             if (V::ok(s)) {
                 const int i = V::idx(s);
                 double jx = 0.0;
-                for (int j = 0; j < N; ++j) jx = fma(J[i + N * j], buf[j], jx);
+                for (int j = 0; j < N; ++j) jx = fma(__ldcg(J + i + N * j), buf[j], jx);
                 r[s] = b[s] - (g * x[s] - jx);
             }
         }

@@ -80,6 +80,12 @@ def parse():
     p.add_argument("--acc-sample", type=int, default=1024,
                    help="systems compared with the rtol-1e-12 oracle after the timed steps (0: none)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ref-gpu-sample", type=int, default=0,
+                   help="systems the reference's own GPU Radau integrates over the first global step from t=0 "
+                        "(0: skip).  One thread per system runs its whole integration, so the launch lasts as "
+                        "long as its slowest system (minutes at 53 species): size it to one wave, e.g. 65536")
+    p.add_argument("--no-config1", action="store_true",
+                   help="skip the van der Pol line (131,072 ICs, t = 0 -> 1 in 100 steps)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--queue-order", type=int, default=3, choices=[-1, 0, 1, 2, 3],
@@ -316,6 +322,89 @@ def run_reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- reference GPU kernel
+def reference_gpu_leg(args, mech, y, var, first_tuned, first_plain):
+    """The reference's own GPU Radau (oracle/_ref, radau2a.cu under intDriver, one thread per
+    system).  As shipped it fails every system (its error estimate solves with the raw
+    Jacobian, radau2a.cu:612): that is recorded on 256 systems.  The throughput is the build
+    with that one line fixed (solve with the factored E1), on the first --ref-gpu-sample
+    systems over the first global step from t=0, compared with the library's own rates on
+    that same global step of the whole batch (first_tuned, first_plain: system-steps/s)."""
+    from oracle import ReferenceGPU, reference_gpu_available
+    if not (reference_gpu_available(54) and reference_gpu_available(54, q3_fix=True)):
+        return None
+    r = ReferenceGPU(54)
+    r.set_mechanism(mech)
+    _, codes0, ms0 = r.run(y[:, :256], var[:256], 0.0, DT, DT)
+    s = min(args.num, args.ref_gpu_sample)
+    r = ReferenceGPU(54, q3_fix=True)
+    r.set_mechanism(mech)
+    t0 = time.time()
+    _, codes, ms = r.run(y[:, :s], var[:s], 0.0, DT, DT)
+    rate = s / (ms / 1000.0)
+    return {"value": rate, "unit": UNIT, "kind": "reference_gpu",
+            "as_shipped": {"systems": 256, "codes": np.bincount(codes0, minlength=5).tolist(), "kernel_ms": ms0,
+                           "note": "every system ends with EC_h_plus_t_equals_h: the error estimate solves "
+                                   "with the raw Jacobian (radau2a.cu:612), a zero diagonal entry makes the "
+                                   "error infinite and the step size zero"},
+            "sample": f"first {s} of the {args.num} systems x the first global step from t=0; the "
+                      "reference's radau2a.cu with its error-estimate line fixed (E1 = solver->E1), under "
+                      "intDriver (one thread per system, 64-thread blocks, strict IEEE flags), built for "
+                      f"sm_100a; summed CUDA-event time of its launches ({ms / 1000.0:.1f} s, "
+                      f"{time.time() - t0:.1f} s wall)",
+            "failed_systems": int((codes != 0).sum()),
+            "first_step_tuned": first_tuned, "first_step_plain_fp64": first_plain,
+            "tuned_over_reference_gpu": first_tuned / rate,
+            "plain_fp64_over_reference_gpu": first_plain / rate if first_plain else None}
+
+
+def config1_leg(dev):
+    """Van der Pol (mu = 1000), 131,072 ICs, t = 0 -> 1 in 100 global steps of 1e-2, plain FP64
+    Radau at rtol 1e-6 / atol 1e-10: the library, the reference's GPU kernel and the reference's
+    CPU integrator (all host threads), each over the whole batch."""
+    import torch
+    import accelerint_b200 as A
+    from oracle import Reference, ReferenceGPU, reference_available, reference_gpu_available
+    num, steps = 131072, 100
+    vdp = A.VanDerPol()
+    y, var = A.vdp_initial_conditions(num, seed=1)
+    integ = A.Integrator(num, vdp, device=dev.index)
+    out = {"workload": "van der Pol mu=1000, 131072 ICs y1~U[-2,2] y2~U[-1,1], t 0->1 in 100 steps of 1e-2, "
+                       "radau2a FP64 rtol 1e-6 atol 1e-10"}
+    try:
+        yd = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
+        vd = torch.from_numpy(var).to(dev)
+        integ.integrate_device(0.0, 1e-2, 1e-2, yd[:, :1024].contiguous(), vd[:1024].contiguous())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record()
+        integ.integrate_device(0.0, 1.0, 1e-2, yd, vd)
+        b.record()
+        torch.cuda.synchronize(dev)
+        ours = num * steps / (a.elapsed_time(b) / 1000.0)
+        out["ours"] = {"value": ours, "unit": UNIT, "kernel": "thread per system, one launch for all 100 steps"}
+    finally:
+        integ.close()
+    if reference_gpu_available(2) and reference_gpu_available(2, q3_fix=True):
+        _, codes0, _ = ReferenceGPU(2).run(y[:, :256], var[:256], 0.0, 1e-2, 1e-2)
+        _, codes, ms = ReferenceGPU(2, q3_fix=True).run(y, var, 0.0, 1.0, 1e-2)
+        rg = num * steps / (ms / 1000.0)
+        out["reference_gpu"] = {"value": rg, "unit": UNIT, "failed_systems": int((codes != 0).sum()),
+                                "ours_over": ours / rg, "build": "error-estimate line fixed (E1 = solver->E1)",
+                                "as_shipped_codes_256": np.bincount(codes0, minlength=5).tolist()}
+    if reference_available("radau2a", 2):
+        ref = Reference("radau2a", 2)
+        nthreads = os.cpu_count() or 1
+        ys = y.copy()
+        t0 = time.time()
+        for k in range(steps):
+            ys, _ = ref.integrate(ys, var, k * 1e-2, (k + 1) * 1e-2, nthreads)
+        el = time.time() - t0
+        rc = num * steps / el
+        out["reference_cpu"] = {"value": rc, "unit": UNIT, "cores": nthreads, "ours_over": ours / rc}
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -539,6 +628,13 @@ def run_ours(args):
                     acc["plain_fp64"] = accuracy(y_plain[:, ok], y_tight[:, ok])
                 if y_ref_cpu is not None and y_ref_cpu.shape[1] >= acc_n:
                     acc["reference_cpu_rtol1e-6"] = accuracy(y_ref_cpu[:, :acc_n][:, ok], y_tight[:, ok])
+        ref_gpu = None
+        if args.ref_gpu_sample > 0:
+            # one GPU against one GPU: rank 0's own batch
+            f_t = args.num / (step_ms[0] / 1000.0)
+            f_p = args.num / (plain["ms_per_global_step"][0] / 1000.0) if plain else None
+            ref_gpu = reference_gpu_leg(args, mech, y, var, f_t, f_p)
+        conf1 = None if args.no_config1 else config1_leg(dev)
         mb = args.num * mech.n_state * 8 / 1e6
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
@@ -556,7 +652,8 @@ def run_ours(args):
                            + ("captured CUDA graph" if not args.no_graph else "direct launch")},
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain, "accuracy": acc,
-                "learned": learn_info, "work": work, "ms_per_global_step": step_ms}
+                "learned": learn_info, "work": work, "ms_per_global_step": step_ms,
+                "reference_gpu": ref_gpu, "config1_van_der_pol": conf1}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist

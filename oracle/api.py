@@ -264,8 +264,9 @@ class Reference:
         return y, codes
 
 
-def reference_gpu_available(n: int) -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", f"libref_gpu_radau2a_n{n}.so"))
+def reference_gpu_available(n: int, q3_fix: bool = False) -> bool:
+    tag = "_q3fix" if q3_fix else ""
+    return os.path.exists(os.path.join(HERE, "_ref", f"libref_gpu_radau2a{tag}_n{n}.so"))
 
 
 class ReferenceGPU:
@@ -273,11 +274,13 @@ class ReferenceGPU:
     intDriver, one thread per system), compiled unmodified by oracle/build.py with the
     mechanism callbacks for state length n (2: the reference's van der Pol example; 54: the
     synthetic mass-action mechanism, oracle/refshim/ma_gpu) and the host entry
-    oracle/refshim/ref_gpu_entry.cu.  Needs a GPU."""
+    oracle/refshim/ref_gpu_entry.cu.  q3_fix: the build whose error estimate solves with
+    the factored E1 (oracle/build.py: Q3_FIX) instead of the raw Jacobian.  Needs a GPU."""
 
-    def __init__(self, n: int):
+    def __init__(self, n: int, q3_fix: bool = False):
         self.n = n
-        self.lib = ctypes.CDLL(os.path.join(HERE, "_ref", f"libref_gpu_radau2a_n{n}.so"))
+        tag = "_q3fix" if q3_fix else ""
+        self.lib = ctypes.CDLL(os.path.join(HERE, "_ref", f"libref_gpu_radau2a{tag}_n{n}.so"))
         self.lib.refgpu_run.restype = ctypes.c_int
         self.lib.refgpu_run.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp,
                                         _ip, _dp]

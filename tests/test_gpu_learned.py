@@ -120,8 +120,9 @@ def test_learned_step_size_gain(trained, oracle):
     ep, el = per_system_error(yp[:, sub], yt), per_system_error(yl[:, sub], yt)
     print(f"error vs tight oracle (median / max): plain {np.median(ep):.3g} / {ep.max():.3g}, "
           f"learned {np.median(el):.3g} / {el.max():.3g}")
-    assert np.median(el) <= 2.0 * np.median(ep) + 1.0
-    assert el.max() <= 2.0 * ep.max() + 1.0
+    # slack of 0.1: a weighted error below 0.1 is a tenth of the tolerance
+    assert np.median(el) <= 2.0 * np.median(ep) + 0.1
+    assert el.max() <= 2.0 * ep.max() + 0.1
 
 
 def test_learned_stage_guess_falls_back_safely(trained):

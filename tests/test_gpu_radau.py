@@ -34,8 +34,11 @@ def test_van_der_pol(oracle, lu):
         # a tight oracle must stay that of the FP64 solver
         yt, _, _ = oracle.run("radau2a", VanDerPol(), y, var, 0.0, 0.1, 1e-2, rtol=1e-12, atol=1e-20)
         eg, eo = per_system_error(yg, yt), per_system_error(yo, yt)
-        assert np.median(eg) <= 2.0 * np.median(eo) + 1.0
-        assert eg.max() <= 3.0 * eo.max() + 1.0
+        print(f"\nvan der Pol lu={lu}: weighted error vs tight median {np.median(eg):.3g} (oracle {np.median(eo):.3g}), "
+              f"max {eg.max():.3g} ({eo.max():.3g})")
+        # slack of 0.1: a weighted error below 0.1 is a tenth of the tolerance
+        assert np.median(eg) <= 2.0 * np.median(eo) + 0.1
+        assert eg.max() <= 3.0 * eo.max() + 0.1
 
 
 def check_mass_action(yg, yo, yp, yt, lu):
@@ -46,8 +49,10 @@ def check_mass_action(yg, yo, yp, yt, lu):
         check_parity(yg, yo, yp)
     eg, eo = per_system_error(yg, yt), per_system_error(yo, yt)
     assert not np.isnan(yg).any()
-    assert np.median(eg) <= 1.5 * np.median(eo) + 1.0
-    assert eg.max() <= 2.0 * eo.max() + 1.0
+    print(f"\nmass action lu={lu}: weighted error vs tight median {np.median(eg):.3g} (oracle {np.median(eo):.3g}), "
+          f"max {eg.max():.3g} ({eo.max():.3g})")
+    assert np.median(eg) <= 1.5 * np.median(eo) + 0.1
+    assert eg.max() <= 2.0 * eo.max() + 0.1
 
 
 @pytest.mark.parametrize("lu", [LU_FP64, LU_FP32, LU_FP32_ALL])
