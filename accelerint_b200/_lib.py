@@ -34,7 +34,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_set_learned", "accelerInt_set_step_recording", "accelerInt_set_graph_launch",
     "accelerInt_set_launch_config", "accelerInt_autotune", "accelerInt_set_persistent",
     "accelerInt_set_queue_order", "accelerInt_set_cost_model", "accelerInt_set_learned_growth_floor",
-    "accelerInt_set_jacobian", "accelerInt_radau_decomp",
+    "accelerInt_set_jacobian", "accelerInt_radau_decomp", "accelerInt_set_mapping", "accelerInt_get_mapping",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -77,6 +77,8 @@ def load_library():
     lib.accelerInt_set_cost_model.argtypes = [vp, vp]
     lib.accelerInt_set_learned_growth_floor.argtypes = [ctypes.c_double]
     lib.accelerInt_set_launch_config.argtypes = [i, i]
+    lib.accelerInt_set_mapping.argtypes = [i, i]
+    lib.accelerInt_get_mapping.argtypes = [vp, vp, vp]
     lib.accelerInt_autotune.argtypes = [i, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, i, vp, vp, vp]
     lib.accelerInt_radau_decomp.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, vp]
     lib.accelerInt_kernel_launches.argtypes = []
@@ -163,6 +165,17 @@ class Integrator:
                                                  var_dev.data_ptr(), int(sample), ctypes.byref(occ),
                                                  ctypes.byref(blk), ctypes.byref(ms)))
         return occ.value & 0xffff, occ.value >> 16, blk.value, ms.value
+
+    def set_mapping(self, team_lanes: int = 0, grain: int = 1):
+        """team_lanes 0: the default team; 16: two systems per warp (state length <= 16).
+        grain: work-queue slots a team claims per atomic."""
+        self._check(self.lib.accelerInt_set_mapping(int(team_lanes), int(grain)))
+
+    def mapping(self):
+        """(team_lanes, grain, resident blocks per SM of the last persistent launch)."""
+        tl, gr, oc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.accelerInt_get_mapping(ctypes.byref(tl), ctypes.byref(gr), ctypes.byref(oc)))
+        return tl.value, gr.value, oc.value
 
     def set_queue_order(self, mode: int):
         self._check(self.lib.accelerInt_set_queue_order(int(mode)))

@@ -95,6 +95,11 @@ struct State {
     // for the persistent team kernels, block size of the thread-per-system kernels
     int occ_cap = 0;
     int tps_block = 128;
+    // team mapping of mass-action Radau: 0 the default team (one warp up to 32 state
+    // elements, two warps up to 64); 16: two systems per warp (16 lanes each), for
+    // state lengths up to 16 (analytic Jacobian, no learned mode)
+    int team_lanes = 0;
+    int grain = 1;                // work-queue slots a team claims per atomic
     int last_occ = 0;             // resident blocks per SM of the last team launch
     bool graph = false;           // device-buffer launches through a captured CUDA graph
     bool persistent = true;       // team kernels: persistent grid + work queue (else one team per system)
@@ -452,13 +457,25 @@ int launch_decomp_prec(int precision, int count, const double* jac, const double
     return launch_decomp<K, TS, float, float>(count, jac, h, e1, e2, perm, info, s);
 }
 
+// Two systems per warp (team_lanes 16) serve analytic-Jacobian Radau without learned
+// proposals; other settings run on the default team.
+bool half_warp_teams(const BatchArgs& a) {
+    return g.team_lanes == 16 && g.solver == ACCELERINT_RADAU2A && g.jac_mode == 0 && !a.learn.mlp.flags &&
+           !a.learn.rec;
+}
+
 int launch(BatchArgs a, cudaStream_t s) {
     if (a.num <= 0) return ACCELERINT_OK;
+    a.grain = g.grain;
     if (g.mech_kind == 0) return launch_vdp(a, s);
     switch (device_species(g.mt.K)) {
-        case 13: return launch_mass_action<13, 32>(a, s);
+        case 13:
+            if (half_warp_teams(a)) return launch_mass_action_padded<13, 16>(a, s);
+            return launch_mass_action<13, 32>(a, s);
         case 53: return launch_mass_action<53, 64>(a, s);
-        case 15: return launch_mass_action_padded<15, 32>(a, s);
+        case 15:
+            if (half_warp_teams(a)) return launch_mass_action_padded<15, 16>(a, s);
+            return launch_mass_action_padded<15, 32>(a, s);
         case 31: return launch_mass_action_padded<31, 32>(a, s);
         case 47: return launch_mass_action_padded<47, 64>(a, s);
         case 63: return launch_mass_action_padded<63, 64>(a, s);
@@ -606,6 +623,8 @@ void accelerInt_cleanup(void) {
     g.cap_stream = nullptr;
     g.occ_cap = 0;
     g.tps_block = 128;
+    g.team_lanes = 0;
+    g.grain = 1;
     g.graph = false;
     g.persistent = true;
     g.jac_mode = 0;
@@ -844,6 +863,20 @@ int accelerInt_set_launch_config(int occupancy_cap, int tps_block) {
     return ACCELERINT_OK;
 }
 
+int accelerInt_set_mapping(int team_lanes, int grain) {
+    if ((team_lanes != 0 && team_lanes != 16) || grain < 1 || grain > 64) return ACCELERINT_ERR_ARGUMENT;
+    g.team_lanes = team_lanes;
+    g.grain = grain;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_get_mapping(int* team_lanes, int* grain, int* occupancy) {
+    if (team_lanes) *team_lanes = g.team_lanes;
+    if (grain) *grain = g.grain;
+    if (occupancy) *occupancy = g.last_occ;
+    return ACCELERINT_OK;
+}
+
 int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, const double* y_dev,
                         const double* var_dev, int sample, int* occupancy_cap_out, int* tps_block_out,
                         double* best_ms_out) {
@@ -918,6 +951,32 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
                 if (ms < best) { best = ms; best_o = o; }
             }
             g.order_mode = best_o;
+        }
+        // mapping: two systems per warp where the state fits 16 lanes (at the
+        // occupancy maximum of that kernel), then the queue granularity
+        if (!rc && g.mech_kind == 1 && g.mt.K + 1 <= 16 && g.solver == ACCELERINT_RADAU2A && g.jac_mode == 0 &&
+            !g.learn.mlp.flags && !g.learn.rec) {
+            const int keep_lanes = g.team_lanes, keep_cap = g.occ_cap;
+            g.team_lanes = 16;
+            g.occ_cap = 0;
+            if (!(rc = trial(&ms)) && ms < best) {
+                best = ms;
+            } else {
+                g.team_lanes = keep_lanes;
+                g.occ_cap = keep_cap;
+            }
+        }
+        if (!rc && g.persistent) {
+            int best_gr = g.grain;
+            for (int gr : {1, 2, 4, 8}) {
+                if (gr == best_gr) continue;
+                const int keep = g.grain;
+                g.grain = gr;
+                if ((rc = trial(&ms))) break;
+                if (ms < best) { best = ms; best_gr = gr; }
+                g.grain = keep;
+            }
+            g.grain = best_gr;
         }
     }
     cudaEventDestroy(e0);

@@ -38,6 +38,7 @@ struct BatchArgs {
     const int* order;       // queue order (system index of each queue slot), or null: index order
     int* cost;              // per-system steps of this call (written), or null
     int n_state;            // the caller's state length (rows of y), when the kernel's N pads it; 0: N
+    int grain;              // queue slots a team claims per atomic (0 or 1: one)
 };
 
 // The reference's global-step loop (generic/solver_main.c:196-209), measured from t_start.
@@ -174,6 +175,9 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
     const int gteam = blockIdx.x * tpb + tib;
     unsigned char* base = smem + size_t(tib) * lay.total;
     const int lane = TM::lane();
+    // queue slots claimed by this team and not yet taken (lane 0's copy counts)
+    const int grain = a.grain > 1 ? a.grain : 1;
+    int next = 0, left = 0;
     for (int it = 0;; ++it) {
         int sys = 0;
         if (a.plain_grid) {
@@ -181,8 +185,14 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             sys = gteam;
         } else {
             if (lane == 0) {
-                sys = atomicAdd(a.queue, 1);
-                if (a.order && sys < a.num) sys = a.order[sys];
+                if (left == 0) {
+                    next = atomicAdd(a.queue, grain);
+                    left = grain;
+                }
+                sys = next++;
+                --left;
+                if (sys >= a.num) sys = a.num;
+                else if (a.order) sys = a.order[sys];
             }
             sys = TM::bcast(sys, 0);
         }

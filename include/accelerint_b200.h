@@ -203,10 +203,21 @@ int accelerInt_set_step_recording(float* rec_dev, int* count_dev, int capacity);
  * t_start) is evaluated for every system on the tensor cores before the launch.
  * Longest-first order shortens the tail of a launch, whose end waits for the
  * slowest system.  Every call of this setter starts the step-count history afresh.
+ * accelerInt_set_mapping: team_lanes 0 runs a mass-action system on the default
+ * team (one warp for state lengths up to 32, two warps up to 64); 16 runs two
+ * systems per warp, 16 lanes each, for state lengths up to 16 (Radau with the
+ * analytic Jacobian and no learned proposals; other settings keep the default
+ * team).  grain: work-queue slots a persistent team claims per atomic (1..64).
+ * Results do not depend on grain; with team_lanes 16 the team reductions run over
+ * 16 lanes, so results agree with the default team to rounding, not bit for bit.
+ * accelerInt_get_mapping: the current team_lanes, grain and the resident blocks
+ * per SM of the last persistent launch.
  * accelerInt_autotune: times the candidate mappings (resident blocks per SM,
- * then queue order 0 / 1; or the thread-per-system block size) on a copy of the
- * first `sample` systems of y_dev for the given interval (y_dev is not modified)
- * and keeps the fastest; reports the choice (occupancy_cap_out: cap | order << 16)
+ * then queue order 0 / 1, then two systems per warp where the state fits 16
+ * lanes, then the queue granularity 1 / 2 / 4 / 8; or the thread-per-system
+ * block size) on a copy of the first `sample` systems of y_dev for the given
+ * interval (y_dev is not modified) and keeps the fastest; reports the choice
+ * (occupancy_cap_out: cap | order << 16; the rest through accelerInt_get_mapping)
  * and its time. */
 int accelerInt_set_graph_launch(int enable);
 /* enable = 1 (default): the team kernels run a persistent grid (resident
@@ -221,6 +232,8 @@ int accelerInt_set_jacobian(int mode);
 int accelerInt_set_queue_order(int mode);
 int accelerInt_set_cost_model(const float* params_dev, const float* norm_dev);
 int accelerInt_set_launch_config(int occupancy_cap, int tps_block);
+int accelerInt_set_mapping(int team_lanes, int grain);
+int accelerInt_get_mapping(int* team_lanes, int* grain, int* occupancy);
 int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, const double* y_dev,
                         const double* var_dev, int sample, int* occupancy_cap_out, int* tps_block_out,
                         double* best_ms_out);

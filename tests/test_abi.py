@@ -84,6 +84,15 @@ def test_extension_setters_validate_without_a_device():
     assert lib.accelerInt_set_jacobian(0) == 0
     assert lib.accelerInt_set_launch_config(-1, 0) == -1
     assert lib.accelerInt_set_launch_config(0, 48) == -1
+    # mapping: team lanes 0 or 16, queue grain 1..64
+    assert lib.accelerInt_set_mapping(8, 1) == -1
+    assert lib.accelerInt_set_mapping(0, 0) == -1
+    assert lib.accelerInt_set_mapping(0, 65) == -1
+    assert lib.accelerInt_set_mapping(16, 4) == 0
+    tl, gr = ctypes.c_int(), ctypes.c_int()
+    assert lib.accelerInt_get_mapping(ctypes.byref(tl), ctypes.byref(gr), None) == 0
+    assert (tl.value, gr.value) == (16, 4)
+    assert lib.accelerInt_set_mapping(0, 1) == 0
     # learned proposals: unknown flags, missing buffers, not initialised
     assert lib.accelerInt_set_learned(None, None, 4) == -1
     assert lib.accelerInt_set_learned(None, None, 1) == -1
