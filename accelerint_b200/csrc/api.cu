@@ -929,6 +929,16 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
         // persistent teams: resident blocks per SM, from the occupancy maximum down to half of it
         g.occ_cap = 0;
         rc = trial(&ms);   // also measures the maximum
+        // fewer than 8 systems per resident team time the slowest system rather than
+        // the mapping: grow the sample (up to NUM) and measure again
+        const int want = std::min(NUM, 8 * g.last_occ * g.num_sms);
+        if (!rc && want > sample) {
+            cudaFree(ys);
+            ys = nullptr;
+            sample = want;
+            CK(cudaMalloc(&ys, size_t(sample) * N * sizeof(double)));
+            rc = trial(&ms);
+        }
         int best_c = 0;
         if (!rc) {
             best = ms;

@@ -77,6 +77,7 @@ constexpr double ELO = 4;
 // L1 is the precision of E1 (the matrix of the error estimate), LT that of E2.
 template <int N, typename LT, typename L1 = LT> struct RadauRegStore {
     using E1T = L1;
+    static constexpr bool jac_global = false;   // J is the thread's own (local) array
     double J[N * N];
     L1 E1[N * N];
     cx<LT> E2[N * N];
@@ -99,6 +100,7 @@ template <int N, typename LT, typename L1 = LT> struct RadauRegStore {
 // L1 is the precision of E1 (the matrix of the error estimate), LT that of E2.
 template <int N, typename LT, typename L1 = LT> struct RadauTeamStore {
     using E1T = L1;
+    static constexpr bool jac_global = true;    // J is global scratch
     double* J;        // N*N (global scratch)
     L1* E1;           // N*N
     cx<LT>* E2;       // N*N (also the Jacobian evaluation scratch)
@@ -139,6 +141,14 @@ struct RadauParams {
 // stage proposals (which hold three more state vectors per thread)
 template <int N, int TS, class Mech, typename LT, class Store, int LEARN = 0>
 struct Radau {
+    // A Jacobian entry: from L2 (ld.global.cg) when J is global scratch, which a
+    // mechanism may have written with reductions that an L1 line kept from an
+    // earlier read would miss; a plain load when J is the thread's own local
+    // array (ld.global is not valid on a local address).
+    __device__ __forceinline__ static double jload(const double* p) {
+        if constexpr (Store::jac_global) return __ldcg(p);
+        else return *p;
+    }
     using V = Vec<N, TS>;
     using TM = Team<TS>;
     static_assert(!LEARN || TM::block, "learned mode runs on block teams");
@@ -228,7 +238,7 @@ struct Radau {
                 for (int j0 = 0; j0 < NC; j0 += 8) {
                     double v[8];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) v[c] = (j0 + c < N) ? -__ldcg(J + i + (j0 + c) * N) : 0.0;
+                    for (int c = 0; c < 8; ++c) v[c] = (j0 + c < N) ? -jload(J + i + (j0 + c) * N) : 0.0;
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
                         const int j = j0 + c;
@@ -240,7 +250,7 @@ struct Radau {
         } else {
             for (int e = lane; e < N * NC; e += TS) {
                 const int i = e % N, j = e / N;
-                const double mj = j < N ? -__ldcg(J + e) : 0.0;
+                const double mj = j < N ? -jload(J + e) : 0.0;
                 E1[e] = L1(i == j ? mj + g : mj);
                 E2[e] = cx<LT>{LT(i == j ? mj + ar : mj), LT(i == j ? ai : 0.0)};
             }
@@ -256,7 +266,8 @@ struct Radau {
                 // E2 pivots on warp 1 overlapped with E1 on warp 0, E2 updates on both
                 const int2 ii = tlu_pair<N, L1, cx<LT>>(E1, st.perm1(), st.dinv1(), E2, st.perm2(), st.dinv2(), inf);
                 TM::sync();
-                if (l0 && w == 0) { inf[0] = ii.x; inf[1] = ii.y; }
+                // E1's info is known on warp 0, E2's on warp 1 (which pivots it)
+                if (l0) inf[w] = w == 0 ? ii.x : ii.y;
             } else if (TS > 64) {
                 if (w == 0) {
                     const int i1 = wlu_real<N, L1>(E1, st.perm1(), st.dinv1());
@@ -361,7 +372,7 @@ struct Radau {
                 // four partial sums: the Jacobian loads are issued together
                 double a[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-                for (int j = 0; j < N; ++j) a[j & 3] = fma(__ldcg(J + t + N * j), buf[j], a[j & 3]);
+                for (int j = 0; j < N; ++j) a[j & 3] = fma(jload(J + t + N * j), buf[j], a[j & 3]);
                 jx = (a[0] + a[1]) + (a[2] + a[3]);
             }
             V r;
@@ -393,7 +404,7 @@ struct Radau {
             if (V::ok(s)) {
                 const int i = V::idx(s);
                 double jx = 0.0;
-                for (int j = 0; j < N; ++j) jx = fma(__ldcg(J + i + N * j), buf[j], jx);
+                for (int j = 0; j < N; ++j) jx = fma(jload(J + i + N * j), buf[j], jx);
                 r[s] = b[s] - (g * x[s] - jx);
             }
         }

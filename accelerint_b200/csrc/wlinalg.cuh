@@ -11,6 +11,7 @@
 // holds one copy of each: a fully inlined integrator does not fit the
 // instruction cache.
 #pragma once
+#include <type_traits>
 #include "common.cuh"
 
 namespace aib {
@@ -484,6 +485,203 @@ __device__ __noinline__ int2 tlu_pair(T1* A1, int* perm1, T1* dinv1, T2* A2, int
                         if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = efnma(l[r], u[c], a[r][c]);
             }
         }
+        __syncthreads();
+    }
+    return make_int2(info1, info2);
+}
+
+// ---------------------------------------------------------------- balanced two-warp LU
+// Pivot and multipliers of column k of A by one warp: the first maximal |a| (or
+// |Re a| + |Im a|) at or below the diagonal, rows k and p exchanged in column k,
+// the entries below the diagonal scaled by the reciprocal pivot (xGETF2).  Lane 0
+// records the pivot row in *xp (k for a zero pivot), 1/pivot in dinv[k] and the
+// exchange in perm.  Returns info updated for a zero pivot.
+template <int N, typename T>
+__device__ __forceinline__ int tlu_column(T* A, int k, int* perm, T* dinv, int* xp, int info, int lane)
+{
+    constexpr int R = (N + 31) / 32;
+    const T z = ezero_value<T>();
+    double best = -1.0;
+    int bi = 0x7fffffff;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        if (i >= k && i < N) {
+            const double a = emag(A[i + k * N]);
+            if (!(a <= best)) { best = a; bi = i; }
+        }
+    }
+    int p = warp_pivot(best, bi);
+    const T piv = A[p + k * N];
+    const bool nz = !ezero(piv);
+    T rc = z;
+    if (nz) rc = erecip(piv);
+    else { if (info == 0) info = k + 1; p = k; }
+    const T akk = A[k + k * N];
+    T nv[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        T a = z;
+        if (i == k) a = nz ? piv : akk;
+        else if (i > k && i < N) {
+            a = (i == p) ? akk : A[i + k * N];
+            if (nz) a = emul(a, rc);
+        }
+        nv[r] = a;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        if (i >= k && i < N) A[i + k * N] = nv[r];
+    }
+    if (lane == 0) {
+        *xp = p;
+        dinv[k] = nz ? rc : z;
+        if (p != k) { const int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
+    }
+    return info;
+}
+
+// Step k's interchange of rows k and p and rank-1 update, on the columns
+// j = 2 m + w (j > k) that warp w owns; the multipliers (column k) are final.
+template <int N, typename T>
+__device__ __forceinline__ void tlu_update(T* A, int k, int p, int w, int lane)
+{
+    constexpr int R = (N + 31) / 32;
+    constexpr int CB = 4;
+    constexpr int MH = lu_cols(N) / 2;
+    static_assert(MH % CB == 0, "column padding");
+    if (p != k) {
+        const int j = 2 * lane + w;
+        if (j < N && j != k) {
+            const T t = A[k + j * N];
+            A[k + j * N] = A[p + j * N];
+            A[p + j * N] = t;
+        }
+        __syncwarp();
+    }
+    const T z = ezero_value<T>();
+    T l[R];
+    bool act[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = lane + 32 * r;
+        act[r] = i > k && i < N;
+        l[r] = act[r] ? A[i + k * N] : z;
+    }
+    const int mfirst = (k + 1 - w + 1) >> 1;
+    if constexpr (std::is_same<T, cx<float>>::value && R == 2) {
+        // single-precision complex: two packed FP32x2 FMAs per element
+        float2 nlr[R], lim[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            nlr[r] = make_float2(-l[r].re, -l[r].re);
+            lim[r] = make_float2(l[r].im, -l[r].im);
+        }
+        float2* colp = reinterpret_cast<float2*>(A) + lane;
+        const float2* rowk = reinterpret_cast<const float2*>(A) + k;
+#pragma unroll 1
+        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
+            float2 u[CB], us[CB], a[R][CB];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                const int j = 2 * (m0 + c) + w;
+                u[c] = (j > k) ? rowk[j * N] : make_float2(0.f, 0.f);
+                us[c] = make_float2(u[c].y, u[c].x);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < CB; ++c)
+                    a[r][c] = act[r] ? colp[32 * r + (2 * (m0 + c) + w) * N] : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < CB; ++c)
+                    if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = cfnma2(nlr[r], lim[r], u[c], us[c], a[r][c]);
+        }
+    } else if constexpr (std::is_same<T, float>::value && R == 2) {
+        // single-precision real: the lane's two rows as one packed FP32x2 FMA per column
+        const float2 nl = make_float2(-float(l[0]), -float(l[1]));
+        float* colp = reinterpret_cast<float*>(A) + lane;
+        const float* rowk = reinterpret_cast<const float*>(A) + k;
+#pragma unroll 1
+        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
+            float u[CB], a[R][CB];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                const int j = 2 * (m0 + c) + w;
+                u[c] = (j > k) ? rowk[j * N] : 0.f;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < CB; ++c) a[r][c] = act[r] ? colp[32 * r + (2 * (m0 + c) + w) * N] : 0.f;
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                const float2 v = __ffma2_rn(nl, make_float2(u[c], u[c]), make_float2(a[0][c], a[1][c]));
+                a[0][c] = v.x;
+                a[1][c] = v.y;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < CB; ++c)
+                    if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = a[r][c];
+        }
+    } else {
+        T* colp = A + lane;
+#pragma unroll 1
+        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
+            T u[CB], a[R][CB];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                const int j = 2 * (m0 + c) + w;
+                u[c] = (j > k) ? A[k + j * N] : z;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < CB; ++c) a[r][c] = act[r] ? colp[32 * r + (2 * (m0 + c) + w) * N] : z;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int c = 0; c < CB; ++c)
+                    if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = efnma(l[r], u[c], a[r][c]);
+        }
+    }
+}
+
+// E1 and E2 together on the two warps of a 64-thread block team, balanced: in
+// elimination step k warp 0 finds the E1 pivot and multipliers while warp 1 does
+// the same for E2; after a block barrier each warp applies both interchanges and
+// both trailing updates to the columns it owns (j % 2 == warp), and a second
+// barrier closes the step.  The arithmetic per element is that of tlu_pair (the
+// factors are identical); the E1 update is split over both warps instead of
+// running on warp 0 alone.  xchg: two shared ints (the pivot rows).  Each warp
+// returns the info of the matrix it pivots (warp 0: E1 in .x, warp 1: E2 in .y).
+template <int N, typename T1, typename T2>
+__device__ __noinline__ int2 tlu_pair_balanced(T1* A1, int* perm1, T1* dinv1, T2* A2, int* perm2, T2* dinv2,
+                                               int* xchg)
+{
+    const int lane = threadIdx.x & 31;
+    const int w = (threadIdx.x >> 5) & 1;
+    int info1 = 0, info2 = 0;
+    for (int i = lane; i < N; i += 32) {
+        if (w == 0) perm1[i] = i;
+        else perm2[i] = i;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int k = 0; k < N; ++k) {
+        if (w == 0) info1 = tlu_column<N, T1>(A1, k, perm1, dinv1, xchg, info1, lane);
+        else info2 = tlu_column<N, T2>(A2, k, perm2, dinv2, xchg + 1, info2, lane);
+        __syncthreads();
+        const int p1 = xchg[0], p2 = xchg[1];
+        tlu_update<N, T1>(A1, k, p1, w, lane);
+        tlu_update<N, T2>(A2, k, p2, w, lane);
         __syncthreads();
     }
     return make_int2(info1, info2);

@@ -59,6 +59,14 @@ sys.path.insert(0, ROOT)
 
 from accelerint_b200 import mechanism as M  # noqa: E402
 
+T_START = time.time()
+
+
+def phase(name):
+    """Progress of the run on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.time() - T_START:7.1f} s] {name}", file=sys.stderr, flush=True)
+
+
 DT = 1e-6
 METRIC = "ODE systems/s per Δt step, 53-species Radau: tuned vs plain FP64 at rtol 1e-6"
 UNIT = "system-steps/s"
@@ -86,6 +94,13 @@ def parse():
                         "long as its slowest system (minutes at 53 species): size it to one wave, e.g. 65536")
     p.add_argument("--no-config1", action="store_true",
                    help="skip the van der Pol line (131,072 ICs, t = 0 -> 1 in 100 steps)")
+    p.add_argument("--no-config2", action="store_true",
+                   help="skip the 13-species lines (262,144 ICs; radau2a, exprb43, rkc)")
+    p.add_argument("--config2-steps", type=int, default=2,
+                   help="global steps of 1e-6 s from t=0 in the 13-species lines (the configuration runs 1000)")
+    p.add_argument("--config2-rkc", action="store_true", help="time RKC in the 13-species lines too")
+    p.add_argument("--config2-cpu-sample", type=int, default=2048,
+                   help="systems of the 13-species batch the reference CPU solvers integrate")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--queue-order", type=int, default=3, choices=[-1, 0, 1, 2, 3],
@@ -405,6 +420,66 @@ def config1_leg(dev):
     return out
 
 
+def config2_leg(dev, args):
+    """13-species mechanism (27 reactions), 262,144 ICs (T in [1000, 1600] K, Dirichlet(0.5)
+    mole fractions), plain FP64 radau2a / exprb43 / rkc at rtol 1e-6 / atol 1e-10 over the first
+    --config2-steps global steps of 1e-6 s from t=0: the library over the whole batch (one launch
+    for all steps, CUDA events), and the reference's CPU solver (oracle/_ref, all host threads) on
+    the first --config2-cpu-sample systems of the same batch."""
+    import torch
+    import accelerint_b200 as A
+    from oracle import Reference, reference_available
+    num, steps = 262144, args.config2_steps
+    mech = A.mechanism_13()
+    y, var = A.mass_action_initial_conditions(mech, num, seed=2)
+    yd0 = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
+    vd = torch.from_numpy(np.ascontiguousarray(var)).to(dev)
+    nthreads = os.cpu_count() or 1
+    out = {"workload": f"mass-action 13 species / 27 reactions, {num} ICs T~U[1000,1600] K, "
+                       f"Dirichlet(0.5) mole fractions, {steps} global steps of 1e-6 s from t=0, FP64, "
+                       "rtol 1e-6 atol 1e-10"}
+    solvers = ("radau2a", "exprb43", "rkc") if args.config2_rkc else ("radau2a", "exprb43")
+    if not args.config2_rkc:
+        out["rkc"] = {"skipped": "RKC (an explicit stabilised method) takes tens of thousands of steps of "
+                                 "thousands of stages on the stiffest of these systems in their first "
+                                 "microseconds, on the reference CPU code and on the GPU alike; --config2-rkc "
+                                 "times it"}
+    for solver in solvers:
+        integ = A.Integrator(num, mech, solver=solver, device=dev.index)
+        try:
+            yw = yd0[:, :2048].contiguous()
+            integ.integrate_device(0.0, 1e-8, 1e-8, yw, vd[:2048].contiguous())   # warm-up
+            yd = yd0.clone()
+            codes = torch.zeros(num, dtype=torch.int32, device=dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            a.record()
+            integ.integrate_device(0.0, steps * DT, DT, yd, vd, codes)
+            b.record()
+            torch.cuda.synchronize(dev)
+            ms = a.elapsed_time(b)
+            c = codes.cpu().numpy()
+            line = {"value": num * steps / (ms / 1000.0), "unit": UNIT, "ms": ms,
+                    "codes": np.bincount(c, minlength=6).tolist()}
+        finally:
+            integ.close()
+        if reference_available(solver, 14):
+            s = min(num, args.config2_cpu_sample)
+            ref = Reference(solver, 14)
+            ref.set_mechanism(mech)
+            ys = y[:, :s].copy()
+            t0 = time.time()
+            for k in range(steps):
+                ys, _ = ref.integrate(ys, var[:s], k * DT, (k + 1) * DT, nthreads)
+            el = time.time() - t0
+            rc = s * steps / el
+            line["reference_cpu"] = {"value": rc, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                                     "sample": f"first {s} systems x {steps} global steps ({el:.1f} s)"}
+            line["ours_over_reference_cpu"] = line["value"] / rc
+        out[solver] = line
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -427,6 +502,7 @@ def run_ours(args):
     if rank == 0:
         if not args.no_cpu_baseline:
             cb, y_ref_cpu = cpu_baseline(args, mech, y, var)
+            phase("reference CPU baseline done")
         if acc_n > 0:
             from oracle import oracle_available
             if oracle_available():
@@ -454,6 +530,7 @@ def run_ours(args):
         cost_model = Lm.train_cost(crec, mech.n_state)
         learn_info = dict(learn_info or {}, cost_records=int(crec.shape[0]), cost_holdout_loss=cost_model.history[-1],
                           cost_train_s=time.time() - t0)
+    phase("training done")
     integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu)
     if model is not None:
         model.install(integ, args.learned)
@@ -531,6 +608,7 @@ def run_ours(args):
         wall = time.perf_counter() - t0
         barrier()
     launches = integ.kernel_launches() - launches0
+    phase("timed steps done")
     step_ms = [a.elapsed_time(b) for a, b in evs]
     ms = sum(step_ms)
     t_max = max_over_ranks(ms)
@@ -611,6 +689,7 @@ def run_ours(args):
         if args.plain_steps == args.steps:
             y_plain = yd[:, :acc_n].cpu().numpy()
     integ.close()
+    phase("plain form done")
 
     if rank == 0:
         acc = None
@@ -634,7 +713,10 @@ def run_ours(args):
             f_t = args.num / (step_ms[0] / 1000.0)
             f_p = args.num / (plain["ms_per_global_step"][0] / 1000.0) if plain else None
             ref_gpu = reference_gpu_leg(args, mech, y, var, f_t, f_p)
+        phase("accuracy and reference GPU done")
         conf1 = None if args.no_config1 else config1_leg(dev)
+        phase("van der Pol line done")
+        conf2 = None if args.no_config2 else config2_leg(dev, args)
         mb = args.num * mech.n_state * 8 / 1e6
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
@@ -653,7 +735,7 @@ def run_ours(args):
                 "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cb, "plain_fp64": plain, "accuracy": acc,
                 "learned": learn_info, "work": work, "ms_per_global_step": step_ms,
-                "reference_gpu": ref_gpu, "config1_van_der_pol": conf1}
+                "reference_gpu": ref_gpu, "config1_van_der_pol": conf1, "config2_13_species": conf2}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
