@@ -233,6 +233,10 @@ int upload_mass_action() {
 template <class K> int persistent_grid(K kernel, int block, size_t smem, int num_teams_needed, int teams_per_block,
                                        int* grid) {
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    // the whole carveout for shared memory, whatever cache preference the host set for the
+    // device (the reference's own initialisation sets cudaFuncCachePreferL1 device-wide,
+    // generic/solver_interface.cu:118, which would leave room for one or two teams per SM)
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)));
     int nb = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, smem));
     if (nb <= 0) return ACCELERINT_ERR_UNSUPPORTED;
@@ -443,6 +447,7 @@ int launch_decomp(int count, const double* jac, const double* h, void* e1, void*
     const TeamLayout lay = TeamLayout::radau(N, int(sizeof(LT)), M::smem_rhs(0), M::smem_jac(0), int(sizeof(L1)));
     auto kern = decomp_kernel<M, TS, LT, L1>;
     if (lay.total > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total));
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)));
     kern<<<count, TS, lay.total, s>>>(count, jac, h, static_cast<L1*>(e1), static_cast<cx<LT>*>(e2), perm, info, lay);
     CK(cudaGetLastError());
     g.launches++;

@@ -654,132 +654,6 @@ __device__ __forceinline__ void tlu_update(T* A, int k, int p, int w, int lane)
     }
 }
 
-// Step k's interchanges and rank-1 updates of both single-precision matrices
-// (E1 real, E2 complex) on the columns j = 2 m + w that warp w owns, software-
-// pipelined: the shared-memory loads of the next chunk of CB owned columns of
-// both matrices are issued before the current chunk is updated and stored, so
-// their latency overlaps the packed FP32x2 FMAs.  Same arithmetic per element as
-// tlu_update.  Two rows per lane (33 <= N <= 64).
-template <int N>
-__device__ __forceinline__ void tlu_update_pair_f32(float* A1, cx<float>* A2, int k, int p1, int p2, int w,
-                                                    int lane)
-{
-    constexpr int R = (N + 31) / 32;
-    static_assert(R == 2, "two rows per lane");
-    constexpr int CB = 4;
-    constexpr int MH = lu_cols(N) / 2;
-    static_assert(MH % CB == 0, "column padding");
-    float2* A2f = reinterpret_cast<float2*>(A2);
-    if (p1 != k || p2 != k) {
-        const int j = 2 * lane + w;
-        if (j < N && j != k) {
-            if (p1 != k) {
-                const float t = A1[k + j * N];
-                A1[k + j * N] = A1[p1 + j * N];
-                A1[p1 + j * N] = t;
-            }
-            if (p2 != k) {
-                const float2 t = A2f[k + j * N];
-                A2f[k + j * N] = A2f[p2 + j * N];
-                A2f[p2 + j * N] = t;
-            }
-        }
-        __syncwarp();
-    }
-    bool act[R];
-    float l1[R];
-    float2 nlr[R], lim[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = lane + 32 * r;
-        act[r] = i > k && i < N;
-        l1[r] = act[r] ? A1[i + k * N] : 0.f;
-        const float2 l2 = act[r] ? A2f[i + k * N] : make_float2(0.f, 0.f);
-        nlr[r] = make_float2(-l2.x, -l2.x);
-        lim[r] = make_float2(l2.y, -l2.y);
-    }
-    const float2 nl1 = make_float2(-l1[0], -l1[1]);
-    struct Chunk {
-        float u1[CB], a1[R][CB];
-        float2 u2[CB], a2[R][CB];
-    };
-    auto load = [&](int m0, Chunk& c) {
-#pragma unroll
-        for (int q = 0; q < CB; ++q) {
-            const int j = 2 * (m0 + q) + w;
-            c.u1[q] = (j > k) ? A1[k + j * N] : 0.f;
-            c.u2[q] = (j > k) ? A2f[k + j * N] : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int q = 0; q < CB; ++q) {
-                const int e = lane + 32 * r + (2 * (m0 + q) + w) * N;
-                c.a1[r][q] = act[r] ? A1[e] : 0.f;
-                c.a2[r][q] = act[r] ? A2f[e] : make_float2(0.f, 0.f);
-            }
-    };
-    auto apply = [&](int m0, Chunk& c) {
-#pragma unroll
-        for (int q = 0; q < CB; ++q) {
-            const float2 v = __ffma2_rn(nl1, make_float2(c.u1[q], c.u1[q]), make_float2(c.a1[0][q], c.a1[1][q]));
-            c.a1[0][q] = v.x;
-            c.a1[1][q] = v.y;
-            const float2 us = make_float2(c.u2[q].y, c.u2[q].x);
-#pragma unroll
-            for (int r = 0; r < R; ++r) c.a2[r][q] = cfnma2(nlr[r], lim[r], c.u2[q], us, c.a2[r][q]);
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int q = 0; q < CB; ++q) {
-                const int e = lane + 32 * r + (2 * (m0 + q) + w) * N;
-                if (act[r]) {
-                    A1[e] = c.a1[r][q];
-                    A2f[e] = c.a2[r][q];
-                }
-            }
-    };
-    const int mfirst = (k + 1 - w + 1) >> 1;
-    const int mb = (mfirst / CB) * CB;
-    if (mb >= MH) return;
-    Chunk ca, cb;
-    load(mb, ca);
-#pragma unroll 1
-    for (int m0 = mb; m0 < MH; m0 += 2 * CB) {
-        if (m0 + CB < MH) load(m0 + CB, cb);
-        apply(m0, ca);
-        if (m0 + CB >= MH) break;
-        if (m0 + 2 * CB < MH) load(m0 + 2 * CB, ca);
-        apply(m0 + CB, cb);
-    }
-}
-
-// The balanced factorisation of the single-precision pair with the pipelined
-// update (tlu_update_pair_f32); otherwise as tlu_pair_balanced.
-template <int N>
-__device__ __noinline__ int2 tlu_pair_balanced_f32(float* A1, int* perm1, float* dinv1, cx<float>* A2, int* perm2,
-                                                   cx<float>* dinv2, int* xchg)
-{
-    const int lane = threadIdx.x & 31;
-    const int w = (threadIdx.x >> 5) & 1;
-    int info1 = 0, info2 = 0;
-    for (int i = lane; i < N; i += 32) {
-        if (w == 0) perm1[i] = i;
-        else perm2[i] = i;
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int k = 0; k < N; ++k) {
-        if (w == 0) info1 = tlu_column<N, float>(A1, k, perm1, dinv1, xchg, info1, lane);
-        else info2 = tlu_column<N, cx<float>>(A2, k, perm2, dinv2, xchg + 1, info2, lane);
-        __syncthreads();
-        tlu_update_pair_f32<N>(A1, A2, k, xchg[0], xchg[1], w, lane);
-        __syncthreads();
-    }
-    return make_int2(info1, info2);
-}
-
 // E1 and E2 together on the two warps of a 64-thread block team, balanced: in
 // elimination step k warp 0 finds the E1 pivot and multipliers while warp 1 does
 // the same for E2; after a block barrier each warp applies both interchanges and

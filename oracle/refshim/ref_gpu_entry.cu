@@ -28,6 +28,10 @@ extern "C" int refgpu_run(int num, double t0, double t_end, double dt, double* y
 {
     if (num <= 0) return 0;
     const int padded = (num + TARGET_BLOCK_SIZE - 1) / TARGET_BLOCK_SIZE * TARGET_BLOCK_SIZE;
+    // the reference's initialisation prefers L1 device-wide (generic/solver_interface.cu:118);
+    // the caller's preference is put back on return
+    cudaFuncCache prev = cudaFuncCachePreferNone;
+    if (cudaDeviceGetCacheConfig(&prev) != cudaSuccess) return -2;
     if (cudaDeviceSetCacheConfig(cudaFuncCachePreferL1) != cudaSuccess) return -2;
     mechanism_memory* h_mech = (mechanism_memory*)calloc(1, sizeof(mechanism_memory));
     solver_memory* h_sol = (solver_memory*)calloc(1, sizeof(solver_memory));
@@ -79,5 +83,6 @@ extern "C" int refgpu_run(int num, double t0, double t_end, double dt, double* y
     cleanup_solver(&h_sol, &d_sol);
     free(h_mech);
     free(h_sol);
+    cudaDeviceSetCacheConfig(prev);
     return rc;
 }
