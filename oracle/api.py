@@ -209,6 +209,9 @@ class Reference:
         self.lib.ref_poles.argtypes = [_dp, _dp, _dp, _dp]
         if solver == "radau2a":
             self.lib.ref_fd_eval_jacob.argtypes = [ctypes.c_double, ctypes.c_double, _dp, _dp]
+        self._keep = []
+        # the exponential methods' CF poles and residues (rational_approximant.c:23-44)
+        self.lib.ref_init()
 
     def fd_jacob(self, y, pres, t=0.0):
         """The reference's generic/fd_jacob.c (ATOL 1e-10, RTOL 1e-6) at one state: [N, N]."""
@@ -216,8 +219,6 @@ class Reference:
         out = np.zeros(self.n * self.n)
         self.lib.ref_fd_eval_jacob(t, pres, y.ctypes.data_as(_dp), out.ctypes.data_as(_dp))
         return out.reshape(self.n, self.n, order="F")
-        self._keep = []
-        self.lib.ref_init()
 
     def set_mechanism(self, mech):
         if self.n == 2:

@@ -49,6 +49,25 @@ def test_oracle_matches_reference_live(oracle):
     assert np.array_equal(yr, yo)
 
 
+@pytest.mark.parametrize("solver", ["exprb43", "exp4"])
+def test_reference_exponential_methods_live(solver):
+    """The reference's exponential integrators as the bench drives them (oracle.Reference):
+    constructing one computes its CF poles (rational_approximant.c:23-44), and a run on a
+    golden fixture's inputs reproduces the fixture (made by the same reference build)."""
+    from oracle import Reference, reference_available
+    if not reference_available(solver, 14):
+        pytest.skip("reference build absent")
+    ref = Reference(solver, 14)
+    poles, _ = ref.poles()
+    assert np.all(np.abs(poles) > 1.0)
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", f"ma14_{solver}.npz"))
+    ref.set_mechanism(M.mechanism_13())
+    yr, cr = ref.run(np.array(g["y0"]), np.array(g["var"]), 0.0, float(g["t_end"]), float(g["dt"]), nthreads=1)
+    assert np.array_equal(cr, g["codes"])
+    ok = g["codes"] == 0
+    assert np.array_equal(yr[:, ok], g["y"][:, ok])
+
+
 def test_cf_poles_match_reference_cf():
     """numpy restatement of cf.c (oracle/cf.py) against the reference's cf() with the FFTW
     shim and LAPACK from OpenBLAS; both carry the ill-conditioning of the Hankel SVD + roots."""
