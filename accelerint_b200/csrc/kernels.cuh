@@ -130,7 +130,7 @@ struct TeamLayout {
         // dydt scratch; also holds the MLP input and activations in learned mode
         const int rb = rhs_doubles * 8 > (MLP_D0 + 2 * MLP_D4) * 4 ? rhs_doubles * 8 : (MLP_D0 + 2 * MLP_D4) * 4;
         L.rhs = o; o += al(rb);
-        L.inf = o; o += al(2 * 4);
+        L.inf = o; o += al(4 * 4);   // factorisation status of E1, E2; pivot exchange slots of the LU
         L.total = o;
         return L;
     }
