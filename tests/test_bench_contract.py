@@ -68,3 +68,20 @@ def test_state_features_layout():
     assert x.shape == (5, L.D_IN)
     assert np.allclose(x[:, 0], y[0]) and np.allclose(x[:, 14], -6.0) and np.allclose(x[:, 15], 0.0)
     assert (x[:, 16:] == 0).all()
+
+
+def test_tight_fixture_only_for_its_own_sample():
+    """The committed rtol-1e-12 solution of the default accuracy sample is used only when the
+    run's first 1,024 initial states hash to the ones it was made from, over 20 steps."""
+    sys.path.insert(0, ROOT)
+    import bench
+    if not os.path.exists(bench.TIGHT_FIXTURE):
+        pytest.skip("fixture absent")
+    _, y, _ = bench.workload(1 << 20, 2024, 0)
+    got = bench.tight_fixture(y[:, :1024], 20)
+    assert got is not None and got[0].shape == (54, 1024) and (got[1] == 0).all()
+    assert bench.tight_fixture(y[:, :1024], 3) is None
+    assert bench.tight_fixture(y[:, :512], 20) is None
+    z = y[:, :1024].copy()
+    z[0, 5] += 1e-9
+    assert bench.tight_fixture(z, 20) is None
