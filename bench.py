@@ -96,7 +96,7 @@ def parse():
                    help="skip the van der Pol line (131,072 ICs, t = 0 -> 1 in 100 steps)")
     p.add_argument("--no-config2", action="store_true",
                    help="skip the 13-species lines (262,144 ICs; radau2a, exprb43, rkc)")
-    p.add_argument("--config2-steps", type=int, default=2,
+    p.add_argument("--config2-steps", type=int, default=1,
                    help="global steps of 1e-6 s from t=0 in the 13-species lines (the configuration runs 1000)")
     p.add_argument("--config2-rkc", action="store_true", help="time RKC in the 13-species lines too")
     p.add_argument("--config2-cpu-sample", type=int, default=2048,
