@@ -921,6 +921,9 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
     };
     int rc = ACCELERINT_OK;
     double best = 1e300, ms = 0;
+    // a candidate replaces the current choice only when it is 3 % faster: on a sample the
+    // launch's tail varies by a few per cent from trial to trial
+    constexpr double kKeep = 0.97;
     if (g.mech_kind == 0 && (g.solver == ACCELERINT_RADAU2A || g.solver == ACCELERINT_RKC)) {
         // thread per system: block size
         int best_b = g.tps_block;
@@ -934,9 +937,9 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
         // persistent teams: resident blocks per SM, from the occupancy maximum down to half of it
         g.occ_cap = 0;
         rc = trial(&ms);   // also measures the maximum
-        // fewer than 8 systems per resident team time the slowest system rather than
-        // the mapping: grow the sample (up to NUM) and measure again
-        const int want = std::min(NUM, 8 * g.last_occ * g.num_sms);
+        // a few systems per resident team time the slowest system rather than the
+        // mapping: grow the sample to 16 per team (up to NUM) and measure again
+        const int want = std::min(NUM, 16 * g.last_occ * g.num_sms);
         if (!rc && want > sample) {
             cudaFree(ys);
             ys = nullptr;
@@ -951,7 +954,7 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
             for (int c = mx - 1; c >= std::max(1, (mx + 1) / 2) && !rc; --c) {
                 g.occ_cap = c;
                 if ((rc = trial(&ms))) break;
-                if (ms < best) { best = ms; best_c = c; }
+                if (ms < kKeep * best) { best = ms; best_c = c; }
             }
         }
         g.occ_cap = best_c;
@@ -963,7 +966,7 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
                 if (o == keep) continue;
                 g.order_mode = o;
                 if ((rc = trial(&ms))) break;
-                if (ms < best) { best = ms; best_o = o; }
+                if (ms < kKeep * best) { best = ms; best_o = o; }
             }
             g.order_mode = best_o;
         }
@@ -974,7 +977,7 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
             const int keep_lanes = g.team_lanes, keep_cap = g.occ_cap;
             g.team_lanes = 16;
             g.occ_cap = 0;
-            if (!(rc = trial(&ms)) && ms < best) {
+            if (!(rc = trial(&ms)) && ms < kKeep * best) {
                 best = ms;
             } else {
                 g.team_lanes = keep_lanes;
@@ -988,7 +991,7 @@ int accelerInt_autotune(int NUM, double t_start, double t_end, double stepsize, 
                 const int keep = g.grain;
                 g.grain = gr;
                 if ((rc = trial(&ms))) break;
-                if (ms < best) { best = ms; best_gr = gr; }
+                if (ms < kKeep * best) { best = ms; best_gr = gr; }
                 g.grain = keep;
             }
             g.grain = best_gr;

@@ -127,6 +127,15 @@ struct Krylov {
     }
 
     // ------------------------------------------------ Hessenberg LU and inverse
+    // cabs(z) > 0, the zero test of the inverse's inner products (complexInverse.c),
+    // without the square root: true when a part is infinite, false when a part is NaN
+    // (and none infinite), else true unless both parts are zero.
+    __device__ __forceinline__ static bool cnonzero(cxd z) {
+        if (isinf(z.re) || isinf(z.im)) return true;
+        if (isnan(z.re) || isnan(z.im)) return false;
+        return z.re != 0.0 || z.im != 0.0;
+    }
+
     // complexInverse.c:35-74: LU with adjacent-row pivoting; thread per column.
     __device__ int hessenberg_lu(int n) {
         cxd* A = s.inv;
@@ -184,10 +193,10 @@ struct Krylov {
                 if (i < j) {
                     const cxd xi = x[i];
                     cxd v = xi;
-                    if (hypot(xi.re, xi.im) > 0.0) v = cmul(xi, A[i + STRIDE * i]);
+                    if (cnonzero(xi)) v = cmul(xi, A[i + STRIDE * i]);
                     for (int k = i + 1; k < j; ++k) {
                         const cxd xk = x[k];
-                        if (hypot(xk.re, xk.im) > 0.0) v = cadd(v, cmul(xk, A[i + STRIDE * k]));
+                        if (cnonzero(xk)) v = cadd(v, cmul(xk, A[i + STRIDE * k]));
                     }
                     acc[r] = cmul(v, mAjj);
                 }
@@ -211,7 +220,7 @@ struct Krylov {
                     cxd v = (i > j) ? cmake(0.0, 0.0) : A[i + STRIDE * j];
                     for (int k = j + 1; k < n; ++k) {
                         const cxd w = s.cw[k];
-                        if (hypot(w.re, w.im) > 0.0) v = cadd(v, cmul(cmake(-w.re, -w.im), A[i + STRIDE * k]));
+                        if (cnonzero(w)) v = cadd(v, cmul(cmake(-w.re, -w.im), A[i + STRIDE * k]));
                     }
                     A[i + STRIDE * j] = v;
                 }

@@ -215,9 +215,10 @@ int accelerInt_set_step_recording(float* rec_dev, int* count_dev, int capacity);
  * accelerInt_autotune: times the candidate mappings (resident blocks per SM,
  * then queue order 0 / 1, then two systems per warp where the state fits 16
  * lanes, then the queue granularity 1 / 2 / 4 / 8; or the thread-per-system
- * block size) on a copy of the first `sample` systems of y_dev (grown to 8 per
+ * block size) on a copy of the first `sample` systems of y_dev (grown to 16 per
  * resident team, at most NUM, for the team kernels) for the given interval
- * (y_dev is not modified) and keeps the fastest; reports the choice
+ * (y_dev is not modified) and keeps the fastest (a candidate must beat the current
+ * choice by 3 %); reports the choice
  * (occupancy_cap_out: cap | order << 16; the rest through accelerInt_get_mapping)
  * and its time. */
 int accelerInt_set_graph_launch(int enable);
