@@ -263,21 +263,10 @@ struct Radau {
             const int w = TM::warp();
             const bool l0 = (threadIdx.x & 31) == 0;
             if (TS == 64) {
-                // E2 pivots on warp 1 overlapped with E1 on warp 0, E2 updates on both.  Measured
-                // in isolation (N = 54, one factorisation pair per 64-thread block): in FP32_ALL
-                // the two-column panel (each trailing element loaded and stored once per two
-                // steps) is 1.15-1.22x faster than the overlapped split, with the same pivots;
-                // with E1 in FP64 and E2 in FP32 the balanced split (both updates on both warps)
-                // is 1.11x faster with identical factors; in FP64 the overlapped split is kept
-                int2 ii;
-                if constexpr (sizeof(L1) == 4 && sizeof(LT) == 4 && N > 32)
-                    ii = tlu_pair_panel2<N>(reinterpret_cast<float*>(E1), st.perm1(), reinterpret_cast<float*>(st.dinv1()),
-                                            reinterpret_cast<cx<float>*>(E2), st.perm2(),
-                                            reinterpret_cast<cx<float>*>(st.dinv2()), inf);
-                else if constexpr (sizeof(L1) == 8 && sizeof(LT) == 4)
-                    ii = tlu_pair_balanced<N, L1, cx<LT>>(E1, st.perm1(), st.dinv1(), E2, st.perm2(), st.dinv2(), inf);
-                else
-                    ii = tlu_pair<N, L1, cx<LT>>(E1, st.perm1(), st.dinv1(), E2, st.perm2(), st.dinv2(), inf);
+                // E2 pivots on warp 1 overlapped with E1 on warp 0, E2 updates on both.  A
+                // two-column panel form, 1.15-1.22x faster alone, ran the FP32_ALL integrator 6 %
+                // slower on identical work, so this overlapped split serves every precision
+                const int2 ii = tlu_pair<N, L1, cx<LT>>(E1, st.perm1(), st.dinv1(), E2, st.perm2(), st.dinv2(), inf);
                 TM::sync();
                 // E1's info is known on warp 0, E2's on warp 1 (which pivots it)
                 if (l0) inf[w] = w == 0 ? ii.x : ii.y;

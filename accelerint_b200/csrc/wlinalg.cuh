@@ -11,7 +11,6 @@
 // holds one copy of each: a fully inlined integrator does not fit the
 // instruction cache.
 #pragma once
-#include <type_traits>
 #include "common.cuh"
 
 namespace aib {
@@ -485,395 +484,6 @@ __device__ __noinline__ int2 tlu_pair(T1* A1, int* perm1, T1* dinv1, T2* A2, int
                         if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = efnma(l[r], u[c], a[r][c]);
             }
         }
-        __syncthreads();
-    }
-    return make_int2(info1, info2);
-}
-
-// ---------------------------------------------------------------- balanced two-warp LU
-// Pivot and multipliers of column k of A by one warp: the first maximal |a| (or
-// |Re a| + |Im a|) at or below the diagonal, rows k and p exchanged in column k,
-// the entries below the diagonal scaled by the reciprocal pivot (xGETF2).  Lane 0
-// records the pivot row in *xp (k for a zero pivot), 1/pivot in dinv[k] and the
-// exchange in perm.  Returns info updated for a zero pivot.
-template <int N, typename T>
-__device__ __forceinline__ int tlu_column(T* A, int k, int* perm, T* dinv, int* xp, int info, int lane)
-{
-    constexpr int R = (N + 31) / 32;
-    const T z = ezero_value<T>();
-    double best = -1.0;
-    int bi = 0x7fffffff;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = lane + 32 * r;
-        if (i >= k && i < N) {
-            const double a = emag(A[i + k * N]);
-            if (!(a <= best)) { best = a; bi = i; }
-        }
-    }
-    int p = warp_pivot(best, bi);
-    const T piv = A[p + k * N];
-    const bool nz = !ezero(piv);
-    T rc = z;
-    if (nz) rc = erecip(piv);
-    else { if (info == 0) info = k + 1; p = k; }
-    const T akk = A[k + k * N];
-    T nv[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = lane + 32 * r;
-        T a = z;
-        if (i == k) a = nz ? piv : akk;
-        else if (i > k && i < N) {
-            a = (i == p) ? akk : A[i + k * N];
-            if (nz) a = emul(a, rc);
-        }
-        nv[r] = a;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = lane + 32 * r;
-        if (i >= k && i < N) A[i + k * N] = nv[r];
-    }
-    if (lane == 0) {
-        *xp = p;
-        dinv[k] = nz ? rc : z;
-        if (p != k) { const int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
-    }
-    return info;
-}
-
-// Step k's interchange of rows k and p and rank-1 update, on the columns
-// j = 2 m + w (j > k) that warp w owns; the multipliers (column k) are final.
-template <int N, typename T>
-__device__ __forceinline__ void tlu_update(T* A, int k, int p, int w, int lane)
-{
-    constexpr int R = (N + 31) / 32;
-    constexpr int CB = 4;
-    constexpr int MH = lu_cols(N) / 2;
-    static_assert(MH % CB == 0, "column padding");
-    if (p != k) {
-        const int j = 2 * lane + w;
-        if (j < N && j != k) {
-            const T t = A[k + j * N];
-            A[k + j * N] = A[p + j * N];
-            A[p + j * N] = t;
-        }
-        __syncwarp();
-    }
-    const T z = ezero_value<T>();
-    T l[R];
-    bool act[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = lane + 32 * r;
-        act[r] = i > k && i < N;
-        l[r] = act[r] ? A[i + k * N] : z;
-    }
-    const int mfirst = (k + 1 - w + 1) >> 1;
-    if constexpr (std::is_same<T, cx<float>>::value && R == 2) {
-        // single-precision complex: two packed FP32x2 FMAs per element
-        float2 nlr[R], lim[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            nlr[r] = make_float2(-l[r].re, -l[r].re);
-            lim[r] = make_float2(l[r].im, -l[r].im);
-        }
-        float2* colp = reinterpret_cast<float2*>(A) + lane;
-        const float2* rowk = reinterpret_cast<const float2*>(A) + k;
-#pragma unroll 1
-        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
-            float2 u[CB], us[CB], a[R][CB];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const int j = 2 * (m0 + c) + w;
-                u[c] = (j > k) ? rowk[j * N] : make_float2(0.f, 0.f);
-                us[c] = make_float2(u[c].y, u[c].x);
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c)
-                    a[r][c] = act[r] ? colp[32 * r + (2 * (m0 + c) + w) * N] : make_float2(0.f, 0.f);
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c)
-                    if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = cfnma2(nlr[r], lim[r], u[c], us[c], a[r][c]);
-        }
-    } else if constexpr (std::is_same<T, float>::value && R == 2) {
-        // single-precision real: the lane's two rows as one packed FP32x2 FMA per column
-        const float2 nl = make_float2(-float(l[0]), -float(l[1]));
-        float* colp = reinterpret_cast<float*>(A) + lane;
-        const float* rowk = reinterpret_cast<const float*>(A) + k;
-#pragma unroll 1
-        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
-            float u[CB], a[R][CB];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const int j = 2 * (m0 + c) + w;
-                u[c] = (j > k) ? rowk[j * N] : 0.f;
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c) a[r][c] = act[r] ? colp[32 * r + (2 * (m0 + c) + w) * N] : 0.f;
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const float2 v = __ffma2_rn(nl, make_float2(u[c], u[c]), make_float2(a[0][c], a[1][c]));
-                a[0][c] = v.x;
-                a[1][c] = v.y;
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c)
-                    if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = a[r][c];
-        }
-    } else {
-        T* colp = A + lane;
-#pragma unroll 1
-        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
-            T u[CB], a[R][CB];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const int j = 2 * (m0 + c) + w;
-                u[c] = (j > k) ? A[k + j * N] : z;
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c) a[r][c] = act[r] ? colp[32 * r + (2 * (m0 + c) + w) * N] : z;
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c)
-                    if (act[r]) colp[32 * r + (2 * (m0 + c) + w) * N] = efnma(l[r], u[c], a[r][c]);
-        }
-    }
-}
-
-// E1 and E2 together on the two warps of a 64-thread block team, balanced: in
-// elimination step k warp 0 finds the E1 pivot and multipliers while warp 1 does
-// the same for E2; after a block barrier each warp applies both interchanges and
-// both trailing updates to the columns it owns (j % 2 == warp), and a second
-// barrier closes the step.  The arithmetic per element is that of tlu_pair (the
-// factors are identical); the E1 update is split over both warps instead of
-// running on warp 0 alone.  xchg: two shared ints (the pivot rows).  Each warp
-// returns the info of the matrix it pivots (warp 0: E1 in .x, warp 1: E2 in .y).
-template <int N, typename T1, typename T2>
-__device__ __noinline__ int2 tlu_pair_balanced(T1* A1, int* perm1, T1* dinv1, T2* A2, int* perm2, T2* dinv2,
-                                               int* xchg)
-{
-    const int lane = threadIdx.x & 31;
-    const int w = (threadIdx.x >> 5) & 1;
-    int info1 = 0, info2 = 0;
-    for (int i = lane; i < N; i += 32) {
-        if (w == 0) perm1[i] = i;
-        else perm2[i] = i;
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int k = 0; k < N; ++k) {
-        if (w == 0) info1 = tlu_column<N, T1>(A1, k, perm1, dinv1, xchg, info1, lane);
-        else info2 = tlu_column<N, T2>(A2, k, perm2, dinv2, xchg + 1, info2, lane);
-        __syncthreads();
-        const int p1 = xchg[0], p2 = xchg[1];
-        tlu_update<N, T1>(A1, k, p1, w, lane);
-        tlu_update<N, T2>(A2, k, p2, w, lane);
-        __syncthreads();
-    }
-    return make_int2(info1, info2);
-}
-
-// ---------------------------------------------------------------- two-column panel LU
-// Row interchange (k <-> p) on the columns j = 2 m + w that warp w owns, except
-// the columns skip0 and skip1.
-template <int N, typename T>
-__device__ __forceinline__ void tlu_swap_owned(T* A, int k, int p, int w, int lane, int skip0, int skip1)
-{
-    if (p == k) return;
-    const int j = 2 * lane + w;
-    if (j < N && j != skip0 && j != skip1) {
-        const T t = A[k + j * N];
-        A[k + j * N] = A[p + j * N];
-        A[p + j * N] = t;
-    }
-}
-
-// a - l u for one element, the arithmetic of tlu_update (packed FP32x2 for the
-// single-precision complex element).
-__device__ __forceinline__ float2 tlu_fnma(float2 nlr, float2 lim, float2 u, float2 a) {
-    return cfnma2(nlr, lim, u, make_float2(u.y, u.x), a);
-}
-
-// Steps k and k+1 of the pair of factorisations (E1 on warp 0, E2 on warp 1 for the
-// pivots; both warps update the columns they own), with each trailing element
-// loaded and stored once for the two steps:
-//   A  pivot and multipliers of column k;
-//   B  interchange k on the owned columns; the owner of column k+1 applies step k's
-//      update to that column;
-//   C  pivot and multipliers of column k+1; the pivot warp applies interchange k+1
-//      to the multiplier column k;
-//   D  interchange k+1 on the other owned columns, then for owned columns j > k+1:
-//      row k+1 gets step k's update, rows below get step k's and step k+1's.
-// Every element sees the same FMAs in the same order as in tlu_pair, so the
-// factors are identical.  xchg: four shared ints.  Single-precision pair, two rows
-// per lane.
-template <int N>
-__device__ __noinline__ int2 tlu_pair_panel2(float* A1, int* perm1, float* dinv1, cx<float>* A2, int* perm2,
-                                             cx<float>* dinv2, int* xchg)
-{
-    constexpr int R = (N + 31) / 32;
-    static_assert(R == 2, "two rows per lane");
-    constexpr int CB = 4;
-    constexpr int MH = lu_cols(N) / 2;
-    static_assert(MH % CB == 0, "column padding");
-    const int lane = threadIdx.x & 31;
-    const int w = (threadIdx.x >> 5) & 1;
-    float2* A2f = reinterpret_cast<float2*>(A2);
-    int info1 = 0, info2 = 0;
-    for (int i = lane; i < N; i += 32) {
-        if (w == 0) perm1[i] = i;
-        else perm2[i] = i;
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int k = 0; k < N; k += 2) {
-        // ---- A
-        if (w == 0) info1 = tlu_column<N, float>(A1, k, perm1, dinv1, xchg, info1, lane);
-        else info2 = tlu_column<N, cx<float>>(A2, k, perm2, dinv2, xchg + 1, info2, lane);
-        __syncthreads();
-        const int p1 = xchg[0], p2 = xchg[1];
-        if (k + 1 == N) {
-            tlu_swap_owned<N, float>(A1, k, p1, w, lane, k, k);
-            tlu_swap_owned<N, float2>(A2f, k, p2, w, lane, k, k);
-            __syncthreads();
-            break;
-        }
-        // ---- B
-        tlu_swap_owned<N, float>(A1, k, p1, w, lane, k, k);
-        tlu_swap_owned<N, float2>(A2f, k, p2, w, lane, k, k);
-        __syncwarp();
-        if (w == ((k + 1) & 1)) {
-            const int j = k + 1;
-            const float u1 = A1[k + j * N];
-            const float2 u2 = A2f[k + j * N];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int i = lane + 32 * r;
-                if (i > k && i < N) {
-                    A1[i + j * N] = fmaf(-A1[i + k * N], u1, A1[i + j * N]);
-                    const float2 l = A2f[i + k * N];
-                    A2f[i + j * N] = tlu_fnma(make_float2(-l.x, -l.x), make_float2(l.y, -l.y), u2, A2f[i + j * N]);
-                }
-            }
-        }
-        __syncthreads();
-        // ---- C
-        if (w == 0) {
-            info1 = tlu_column<N, float>(A1, k + 1, perm1, dinv1, xchg + 2, info1, lane);
-            __syncwarp();
-            const int q = xchg[2];
-            if (q != k + 1 && lane == 0) {
-                const float t = A1[k + 1 + k * N];
-                A1[k + 1 + k * N] = A1[q + k * N];
-                A1[q + k * N] = t;
-            }
-        } else {
-            info2 = tlu_column<N, cx<float>>(A2, k + 1, perm2, dinv2, xchg + 3, info2, lane);
-            __syncwarp();
-            const int q = xchg[3];
-            if (q != k + 1 && lane == 0) {
-                const float2 t = A2f[k + 1 + k * N];
-                A2f[k + 1 + k * N] = A2f[q + k * N];
-                A2f[q + k * N] = t;
-            }
-        }
-        __syncthreads();
-        // ---- D
-        const int q1 = xchg[2], q2 = xchg[3];
-        tlu_swap_owned<N, float>(A1, k + 1, q1, w, lane, k, k + 1);
-        tlu_swap_owned<N, float2>(A2f, k + 1, q2, w, lane, k, k + 1);
-        __syncwarp();
-        bool act[R];
-        float2 nl1a, nl1b;       // E1 multipliers of the lane's two rows, columns k and k+1
-        float2 nra[R], lia[R], nrb[R], lib[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int i = lane + 32 * r;
-            act[r] = i > k + 1 && i < N;
-            const float2 la = act[r] ? A2f[i + k * N] : make_float2(0.f, 0.f);
-            const float2 lb = act[r] ? A2f[i + (k + 1) * N] : make_float2(0.f, 0.f);
-            nra[r] = make_float2(-la.x, -la.x);
-            lia[r] = make_float2(la.y, -la.y);
-            nrb[r] = make_float2(-lb.x, -lb.x);
-            lib[r] = make_float2(lb.y, -lb.y);
-        }
-        nl1a = make_float2(act[0] ? -A1[lane + k * N] : 0.f, act[1] ? -A1[lane + 32 + k * N] : 0.f);
-        nl1b = make_float2(act[0] ? -A1[lane + (k + 1) * N] : 0.f, act[1] ? -A1[lane + 32 + (k + 1) * N] : 0.f);
-        // multipliers of row k+1 in column k (after interchange k+1)
-        const float m1 = A1[k + 1 + k * N];
-        const float2 m2 = A2f[k + 1 + k * N];
-        const float2 m2r = make_float2(-m2.x, -m2.x), m2i = make_float2(m2.y, -m2.y);
-        const bool own_k1 = lane == ((k + 1) & 31);
-        const int r_k1 = (k + 1) >> 5;
-        const int mfirst = (k + 2 - w + 1) >> 1;
-#pragma unroll 1
-        for (int m0 = (mfirst / CB) * CB; m0 < MH; m0 += CB) {
-            float u1[CB], v1[CB], a1[R][CB];
-            float2 u2[CB], v2[CB], a2[R][CB];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const int j = 2 * (m0 + c) + w;
-                const bool on = j > k + 1;
-                u1[c] = on ? A1[k + j * N] : 0.f;
-                v1[c] = on ? A1[k + 1 + j * N] : 0.f;
-                u2[c] = on ? A2f[k + j * N] : make_float2(0.f, 0.f);
-                v2[c] = on ? A2f[k + 1 + j * N] : make_float2(0.f, 0.f);
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c) {
-                    const int e = lane + 32 * r + (2 * (m0 + c) + w) * N;
-                    a1[r][c] = act[r] ? A1[e] : 0.f;
-                    a2[r][c] = act[r] ? A2f[e] : make_float2(0.f, 0.f);
-                }
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                // row k+1 after step k
-                v1[c] = fmaf(-m1, u1[c], v1[c]);
-                v2[c] = tlu_fnma(m2r, m2i, u2[c], v2[c]);
-                float2 x = __ffma2_rn(nl1a, make_float2(u1[c], u1[c]), make_float2(a1[0][c], a1[1][c]));
-                x = __ffma2_rn(nl1b, make_float2(v1[c], v1[c]), x);
-                a1[0][c] = x.x;
-                a1[1][c] = x.y;
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    a2[r][c] = tlu_fnma(nrb[r], lib[r], v2[c], tlu_fnma(nra[r], lia[r], u2[c], a2[r][c]));
-            }
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const int j = 2 * (m0 + c) + w;
-                if (own_k1 && j > k + 1) {
-                    A1[k + 1 + j * N] = v1[c];
-                    A2f[k + 1 + j * N] = v2[c];
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int c = 0; c < CB; ++c) {
-                    const int e = lane + 32 * r + (2 * (m0 + c) + w) * N;
-                    if (act[r]) {
-                        A1[e] = a1[r][c];
-                        A2f[e] = a2[r][c];
-                    }
-                }
-        }
-        (void)r_k1;
         __syncthreads();
     }
     return make_int2(info1, info2);
