@@ -97,7 +97,7 @@ def parse():
     p.add_argument("--no-config2", action="store_true",
                    help="skip the 13-species lines (262,144 ICs; radau2a, exprb43, rkc)")
     p.add_argument("--config2-steps", type=int, default=1,
-                   help="global steps of 1e-6 s from t=0 in the 13-species lines (the configuration runs 1000)")
+                   help="global steps of 1e-6 s from t=0 in the 13-species lines (the full workload runs 1000)")
     p.add_argument("--config2-rkc", action="store_true", help="time RKC in the 13-species lines too")
     p.add_argument("--config2-cpu-sample", type=int, default=2048,
                    help="systems of the 13-species batch the reference CPU solvers integrate")

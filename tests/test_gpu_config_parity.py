@@ -1,8 +1,8 @@
-"""GPU parity and accuracy at the benchmark configurations' shapes, through the C-ABI
+"""GPU parity and accuracy at the benchmark workloads' shapes, through the C-ABI
 (accelerInt_integrate_status), against the oracle (the plain-C restatement of the
 reference's CPU integrators) on the same seeded inputs.
 
-* 53-species mechanism (the north-star workload), 1,024 mixed-stiffness systems
+* 53-species mechanism (the headline workload), 1,024 mixed-stiffness systems
   (both stiffness halves) over three global steps of 1e-6 s, for the plain FP64
   form, the FP32 and FP32_ALL factorisations and the learned step-size proposals.
   - FP64 must agree with the oracle at rtol 1e-6 / atol 1e-10 as closely as the
@@ -17,13 +17,13 @@ reference's CPU integrators) on the same seeded inputs.
     oracle's own error, with no absolute slack: the median within 1.25x, the
     90th percentile within 1.5x, and the share of systems within tolerance of the
     tight solution no lower than the oracle's less 0.02.
-* 13-species mechanism (the second configuration's mechanism), 1,024 systems over
+* 13-species mechanism (27 reactions, the workload of the 262,144-IC runs), 1,024 systems over
   ten global steps of 1e-6 s for radau2a and exprb43, against an envelope of three
   oracle runs on perturbed inputs (the worst system within 3x of it).  RKC is not run at this
   size: in its initial transient some of these systems take the CPU oracle minutes
   each (tens of thousands of RKC steps of thousands of stages); its parity test
   stays tests/test_gpu_krylov.py's small one.
-* Van der Pol at the first configuration's full span, t = 0 -> 1.0 in steps of
+* Van der Pol (mu = 1000) over the full span of its benchmark, t = 0 -> 1.0 in steps of
   1e-2, on 8,192 initial conditions.
 * Mechanisms of other sizes (20 and 40 species), which run on the Radau kernels
   of the next padded size: FP64 within the perturbation envelope of the oracle,
