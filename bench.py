@@ -31,10 +31,19 @@ as "plain_fp64" with the tuned / plain ratio.
 Accuracy (untimed): the first --acc-sample systems (both stiffness halves) of
 the tuned and plain final states, and of the reference CPU radau2a at rtol 1e-6,
 against the oracle integrated at rtol 1e-12 / atol 1e-20 over the same global
-steps; the oracle runs in a separate process on the host cores while the GPU
-works.  Errors use the reference's weighted metric |x - x_ref| / (atol + rtol
+steps: the committed solution tests/golden/tight/bench_ma54_1m_seed2024_20steps.npz
+when the sample and steps are its own (the default sample over 20 steps), else the
+oracle in a separate process on the host cores while the GPU works.  The plain
+form's Newton iterations per step and rejected share are reported beside the
+tuned form's.  Errors use the reference's weighted metric |x - x_ref| / (atol + rtol
 |x_ref|) with atol 1e-10, rtol 1e-6 (logger.py:53-55), and the maximum
 relative error of T and of the mass fractions above 1e-8.
+
+Side lines (after the headline work, untimed by the headline): van der Pol (mu
+= 1000, 131,072 ICs, t = 0 -> 1 in 100 steps) with the reference's GPU kernel and
+CPU code beside ours; the 13-species mechanism (262,144 ICs) for radau2a and
+exprb43 with the reference CPU code beside; optionally the reference GPU kernel
+on the 53-species batch (--ref-gpu-sample).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--lu fp32|fp32_all|fp64] [--num NUM]
@@ -705,6 +714,7 @@ def run_ours(args):
         yw = y0[:, :nw].contiguous()
         pinteg.integrate_device(0.0, dtw, dtw, yw, vd[:nw].contiguous(), None, None, stream)   # warm-up
         yd.copy_(y0)
+        stats.zero_()   # the tuned form's counters were read above; now the plain form's
         pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(args.plain_steps)]
         barrier()
@@ -712,7 +722,7 @@ def run_ours(args):
             for k in range(args.plain_steps):
                 flush.fill_(k & 0xff)
                 pev[k][0].record(stream)
-                pinteg.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, None, None, stream)
+                pinteg.integrate_device(k * DT, (k + 1) * DT, DT, yd, vd, None, stats, stream)
                 pev[k][1].record(stream)
         barrier()
         pstep = [a.elapsed_time(b) for a, b in pev]
@@ -722,8 +732,18 @@ def run_ours(args):
         # tuned over the same global steps
         tms = max_over_ranks(sum(step_ms[:args.plain_steps]))
         tval = ws * args.num * args.plain_steps / (tms / 1000.0)
+        pst = stats.cpu().numpy().astype(np.float64)
+        pwork = {"radau_steps": int(pst[:, 0].sum()), "rejected": int(pst[:, 2].sum()),
+                 "factorisations": int(pst[:, 4].sum()), "newton_iterations": int(pst[:, 5].sum()),
+                 "max_steps_one_system": int(pst[:, 0].max())}
         plain = {"value": pval, "unit": UNIT, "ms_per_step": pms / args.plain_steps, "steps": args.plain_steps,
-                 "tuned_over_plain": tval / pval, "ms_per_global_step": pstep}
+                 "tuned_over_plain": tval / pval, "ms_per_global_step": pstep, "work": pwork,
+                 "newton_iterations_per_step": pwork["newton_iterations"] / max(1, pwork["radau_steps"]),
+                 "rejected_share": pwork["rejected"] / max(1, pwork["radau_steps"])}
+        if args.plain_steps == args.steps:
+            # the precision form's Newton iterations per step and rejected share, against these
+            work["newton_iterations_per_step"] = work["newton_iterations"] / max(1, work["radau_steps"])
+            work["rejected_share"] = work["rejected"] / max(1, work["radau_steps"])
         if args.plain_steps == args.steps:
             y_plain = yd[:, :acc_n].cpu().numpy()
     integ.close()
