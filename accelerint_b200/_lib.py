@@ -35,6 +35,7 @@ EXPORTED_SYMBOLS = [
     "accelerInt_set_launch_config", "accelerInt_autotune", "accelerInt_set_persistent",
     "accelerInt_set_queue_order", "accelerInt_set_cost_model", "accelerInt_set_learned_growth_floor",
     "accelerInt_set_jacobian", "accelerInt_radau_decomp", "accelerInt_set_mapping", "accelerInt_get_mapping",
+    "accelerInt_set_stage_extrapolation",
 ]
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -78,6 +79,7 @@ def load_library():
     lib.accelerInt_set_learned_growth_floor.argtypes = [ctypes.c_double]
     lib.accelerInt_set_launch_config.argtypes = [i, i]
     lib.accelerInt_set_mapping.argtypes = [i, i]
+    lib.accelerInt_set_stage_extrapolation.argtypes = [i]
     lib.accelerInt_get_mapping.argtypes = [vp, vp, vp]
     lib.accelerInt_autotune.argtypes = [i, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, i, vp, vp, vp]
     lib.accelerInt_radau_decomp.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, vp]
@@ -112,13 +114,14 @@ class Integrator:
     """
 
     def __init__(self, num: int, mechanism, solver: str = "radau2a", device: int = 0,
-                 atol: float = 1e-10, rtol: float = 1e-6, lu: int = LU_FP64):
+                 atol: float = 1e-10, rtol: float = 1e-6, lu: int = LU_FP64, stage_extrapolation: int = 0):
         self.lib = load_library()
         self.mechanism = mechanism
         self.n = mechanism.n_state
         self._check(self.lib.accelerInt_set_solver(SOLVERS[solver]))
         self._check(self.lib.accelerInt_set_tolerances(atol, rtol))
         self._check(self.lib.accelerInt_set_lu_precision(lu))
+        self._check(self.lib.accelerInt_set_stage_extrapolation(int(stage_extrapolation)))
         if mechanism.kind == MECH_VAN_DER_POL:
             self._check(self.lib.accelerInt_set_mechanism_van_der_pol())
         else:
@@ -176,6 +179,11 @@ class Integrator:
         tl, gr, oc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self._check(self.lib.accelerInt_get_mapping(ctypes.byref(tl), ctypes.byref(gr), ctypes.byref(oc)))
         return tl.value, gr.value, oc.value
+
+    def set_stage_extrapolation(self, mode: int):
+        """Radau starting values after an accepted step: 0 the reference's (default), 1 the
+        collocation polynomial at all three nodes."""
+        self._check(self.lib.accelerInt_set_stage_extrapolation(int(mode)))
 
     def set_queue_order(self, mode: int):
         self._check(self.lib.accelerInt_set_queue_order(int(mode)))

@@ -100,6 +100,7 @@ struct State {
     // state lengths up to 16 (analytic Jacobian, no learned mode)
     int team_lanes = 0;
     int grain = 1;                // work-queue slots a team claims per atomic
+    int stage_extrap = 0;         // Radau starting values: 0 the reference's, 1 collocation
     int last_occ = 0;             // resident blocks per SM of the last team launch
     bool graph = false;           // device-buffer launches through a captured CUDA graph
     bool persistent = true;       // team kernels: persistent grid + work queue (else one team per system)
@@ -472,6 +473,7 @@ bool half_warp_teams(const BatchArgs& a) {
 int launch(BatchArgs a, cudaStream_t s) {
     if (a.num <= 0) return ACCELERINT_OK;
     a.grain = g.grain;
+    a.stage_extrap = g.stage_extrap;
     if (g.mech_kind == 0) return launch_vdp(a, s);
     switch (device_species(g.mt.K)) {
         case 13:
@@ -630,6 +632,7 @@ void accelerInt_cleanup(void) {
     g.tps_block = 128;
     g.team_lanes = 0;
     g.grain = 1;
+    g.stage_extrap = 0;
     g.graph = false;
     g.persistent = true;
     g.jac_mode = 0;
@@ -865,6 +868,12 @@ int accelerInt_set_launch_config(int occupancy_cap, int tps_block) {
         return ACCELERINT_ERR_ARGUMENT;
     g.occ_cap = occupancy_cap;
     if (tps_block) g.tps_block = tps_block;
+    return ACCELERINT_OK;
+}
+
+int accelerInt_set_stage_extrapolation(int mode) {
+    if (mode != 0 && mode != 1) return ACCELERINT_ERR_ARGUMENT;
+    g.stage_extrap = mode;
     return ACCELERINT_OK;
 }
 
@@ -1176,6 +1185,7 @@ extern "C" int accelerInt_integrate_device_noalloc(int NUM, double t_start, doub
     a.stats = nullptr;
     a.atol = g.atol;
     a.rtol = g.rtol;
+    a.stage_extrap = g.stage_extrap;
     unsigned char* sp = static_cast<unsigned char*>(scratch);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     switch (g.mt.K) {

@@ -39,6 +39,7 @@ struct BatchArgs {
     int* cost;              // per-system steps of this call (written), or null
     int n_state;            // the caller's state length (rows of y), when the kernel's N pads it; 0: N
     int grain;              // queue slots a team claims per atomic (0 or 1: one)
+    int stage_extrap;       // Radau starting values after an accepted step (RadauParams::stage_extrap)
 };
 
 // The reference's global-step loop (generic/solver_main.c:196-209), measured from t_start.
@@ -84,7 +85,8 @@ __global__ void __launch_bounds__(128) tps_kernel(BatchArgs a, Mech mech)
     StepLoop L(a.t_start, a.t_end, a.step);
     if constexpr (SK == SK_RADAU) {
         RadauRegStore<N, LT, L1> store;
-        Radau<N, 1, Mech, LT, RadauRegStore<N, LT, L1>> rad{mech, store, RadauParams{a.atol, a.rtol}, pr, st};
+        Radau<N, 1, Mech, LT, RadauRegStore<N, LT, L1>> rad{mech, store, RadauParams{a.atol, a.rtol, 0, a.stage_extrap},
+                                                            pr, st};
         while (L.more() && code == EC_success) {
             code = rad.integrate(L.t, L.t_next, y);
             L.advance();
@@ -222,7 +224,7 @@ team_kernel(BatchArgs a, Mech mech, TeamLayout lay)
             store.inf = reinterpret_cast<int*>(base + lay.inf);
             const LearnArgs la = a.learn;
             Radau<N, TS, Mech, LT, RadauTeamStore<N, LT, L1>, LEARN> rad{mech, store,
-                                                                         RadauParams{a.atol, a.rtol, nst},
+                                                                         RadauParams{a.atol, a.rtol, nst, a.stage_extrap},
                                                                          pr, st, LEARN ? &la : nullptr};
             while (L.more() && code == EC_success) {
                 code = rad.integrate(L.t, L.t_next, y);

@@ -6,7 +6,8 @@
 // Same control logic, constants and operation sequence as the CPU reference:
 // simplified Newton with the real E1 and complex E2 factorisations, Gustafsson
 // step control, Jacobian / LU reuse (SkipJac / SkipLU), quadratic-interpolant
-// starting values (including the reference's x2 factor in Z3, radau2a.c:312).
+// starting values (by default including the reference's x2 factor in Z3,
+// radau2a.c:312; RadauParams::stage_extrap selects the collocation polynomial).
 // The matrices are factorised in precision LT (double, or float for the
 // precision form where the Newton loop itself refines the solution and the
 // error-estimate solve gets one FP64 refinement step against J).
@@ -135,6 +136,11 @@ struct RadauParams {
     // caller's state length when the mechanism is padded to the next instantiated size
     // (the padding rows stay zero and add nothing to the sums)
     int n_eff = 0;
+    // starting values of the Newton iteration after an accepted step: 0 the reference's
+    // extrapolation (radau2a.c:312 evaluates Z3 with x2 in its outer factor), 1 the
+    // collocation polynomial of the last step evaluated at all three new nodes (x3 in
+    // both factors of Z3, as in Hairer and Wanner's RADAU5)
+    int stage_extrap = 0;
 };
 
 // LEARN (block teams only): 0 off; 1 step-size proposals and step records; 2 also
@@ -549,11 +555,12 @@ struct Radau {
             } else {
                 const double r = H / Hold;
                 const double x1 = 1.0 + radau::C(0) * r, x2 = 1.0 + radau::C(1) * r, x3 = 1.0 + radau::C(2) * r;
+                const double x3o = prm.stage_extrap ? x3 : x2;   // outer factor of Z3
 #pragma unroll
                 for (int s = 0; s < S; ++s) {
                     Z1[s] = CONT0[s] + x1 * (CONT1[s] + x1 * CONT2[s]);
                     Z2[s] = CONT0[s] + x2 * (CONT1[s] + x2 * CONT2[s]);
-                    Z3[s] = CONT0[s] + x2 * (CONT1[s] + x3 * CONT2[s]);
+                    Z3[s] = CONT0[s] + x3o * (CONT1[s] + x3 * CONT2[s]);
                 }
             }
             NewtonDone = false;

@@ -59,13 +59,15 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 
 def record_steps(mech, y, var, t0, t1, dt, capacity: int = 1 << 20, device: int = 0, lu: int = LU_FP64,
-                 solver: str = "radau2a"):
+                 solver: str = "radau2a", stage_extrapolation: int = 0):
     """Run the plain Radau solver on (y, var) and capture one record per accepted step.
+    stage_extrapolation: the solver's starting values (Integrator.set_stage_extrapolation),
+    that of the form the model will serve.
 
     Returns a CUDA float32 tensor [n, 240]: raw features then raw targets."""
     import torch
     num = y.shape[1]
-    integ = Integrator(num, mech, solver=solver, device=device, lu=lu)
+    integ = Integrator(num, mech, solver=solver, device=device, lu=lu, stage_extrapolation=stage_extrapolation)
     try:
         rec = torch.zeros((capacity, REC), dtype=torch.float32, device=f"cuda:{device}")
         cnt = torch.zeros(1, dtype=torch.int32, device=f"cuda:{device}")
@@ -205,12 +207,12 @@ def state_features(y, var, h):
     return x
 
 
-def cost_records(mech, y, var, t0, t1, dt, device: int = 0, lu: int = LU_FP64):
+def cost_records(mech, y, var, t0, t1, dt, device: int = 0, lu: int = LU_FP64, stage_extrapolation: int = 0):
     """One record per system and global step: the state's features at the step start
     and, as output 0, log10(1 + Radau steps the plain solver took in that step)."""
     import torch
     num = y.shape[1]
-    integ = Integrator(num, mech, device=device, lu=lu)
+    integ = Integrator(num, mech, device=device, lu=lu, stage_extrapolation=stage_extrapolation)
     dev = f"cuda:{device}"
     recs = []
     try:

@@ -22,7 +22,10 @@ The tuned form is three changes on top of the plain FP64 form:
 E1/E2 factorised and solved in FP32 (--lu), the persistent work-queue kernel
 under a captured CUDA graph with the autotuned mapping and a longest-first
 queue order from a learned per-system cost model (--queue-order 3), and the
-learned step-size proposals (--learned).  Both networks are trained, untimed,
+stage and step-size proposals: the Newton iteration starts from the collocation
+polynomial evaluated at all three new nodes (--stage-extrapolation 1; the plain
+form keeps the reference's start, radau2a.c:312, for parity) and the learned
+step-size proposals cap the step growth (--learned).  Both networks are trained, untimed,
 by the library's kernels on plain Radau runs of batches drawn with other seeds.
 The plain FP64 form (one team per system over a plain grid, FP64
 factorisations, no proposals) is timed on the same batch and steps and reported
@@ -122,6 +125,9 @@ def parse():
     p.add_argument("--no-graph", action="store_true")
     p.add_argument("--learned", type=int, default=1, choices=[0, 1, 2, 3],
                    help="learned proposals in the tuned form: 1 step size, 2 stages, 3 both (0: off)")
+    p.add_argument("--stage-extrapolation", type=int, default=1, choices=[0, 1],
+                   help="Radau starting values in the tuned form: 1 the collocation polynomial at all three "
+                        "nodes, 0 the reference's (radau2a.c:312, the plain form's)")
     p.add_argument("--growth-floor", type=float, default=2.0,
                    help="learned step-size proposals never hold the step below this x the last accepted")
     p.add_argument("--train-epochs", type=int, default=8)
@@ -562,7 +568,8 @@ def run_ours(args):
         from accelerint_b200 import learned as Lm
         t0 = time.time()
         yt, vt = M.mixed_stiffness_initial_conditions(mech, args.train_num, args.seed + 104729 + rank)
-        rec = Lm.record_steps(mech, yt, vt, 0.0, args.steps * DT, DT, capacity=1 << 22, device=dev.index)
+        rec = Lm.record_steps(mech, yt, vt, 0.0, args.steps * DT, DT, capacity=1 << 22, device=dev.index,
+                              stage_extrapolation=args.stage_extrapolation)
         model = Lm.train(rec, mech.n_state, epochs=args.train_epochs, batch=args.train_batch,
                          lr=2e-3 if args.train_batch >= 4096 else 1e-3)
         learn_info = {"flags": args.learned, "train_systems": args.train_num, "records": int(rec.shape[0]),
@@ -573,12 +580,14 @@ def run_ours(args):
         from accelerint_b200 import learned as Lm
         t0 = time.time()
         yt, vt = M.mixed_stiffness_initial_conditions(mech, 4 * args.train_num, args.seed + 130363 + rank)
-        crec = Lm.cost_records(mech, yt, vt, 0.0, args.steps * DT, DT, device=dev.index, lu=lu)
+        crec = Lm.cost_records(mech, yt, vt, 0.0, args.steps * DT, DT, device=dev.index, lu=lu,
+                               stage_extrapolation=args.stage_extrapolation)
         cost_model = Lm.train_cost(crec, mech.n_state)
         learn_info = dict(learn_info or {}, cost_records=int(crec.shape[0]), cost_holdout_loss=cost_model.history[-1],
                           cost_train_s=time.time() - t0)
     phase("training done")
-    integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu)
+    integ = A.Integrator(args.num, mech, solver=args.solver, device=dev.index, lu=lu,
+                         stage_extrapolation=args.stage_extrapolation)
     if model is not None:
         model.install(integ, args.learned)
         integ.lib.accelerInt_set_learned_growth_floor(args.growth_floor)
@@ -788,7 +797,9 @@ def run_ours(args):
                 "config": {"workload": f"mass-action 53 species / 325 reactions, mixed stiffness, {args.num} ICs "
                                        f"per GPU, global steps of dt=1e-6 s from t=0, {args.solver} rtol 1e-6 "
                                        f"atol 1e-10, LU {args.lu}, persistent work-queue team kernel"
-                                       + (f", learned proposals {args.learned}" if args.learned else ""),
+                                       + (f", learned proposals {args.learned}" if args.learned else "")
+                                       + (", collocation starting values" if args.stage_extrapolation else
+                                          ", the reference's starting values"),
                            "l2": f"L2 flushed (256 MiB write) before every timed step; state y is {mb:.0f} MB",
                            "warmup": f"{args.warmup} global steps of dt/1000 on the whole batch, then reset",
                            "failed_systems": nfail, "nonfinite_systems": nonfinite,

@@ -103,6 +103,14 @@ int accelerInt_set_mechanism_van_der_pol(void);
 int accelerInt_set_mechanism_mass_action(const accelerInt_mass_action* mech);
 int accelerInt_set_tolerances(double atol, double rtol);   /* defaults 1e-10 / 1e-6 */
 int accelerInt_set_lu_precision(int precision);             /* ACCELERINT_LU_FP64 (default) */
+/* Radau IIA starting values of the simplified Newton iteration after an accepted
+ * step (RK_Interpolate, radau2a/radau2a.c:302-314): 0 (default) the reference's,
+ * which evaluates Z3 with x2 in its outer factor (radau2a.c:312), for trajectory
+ * parity with the reference; 1 the collocation polynomial of the last step
+ * evaluated at all three new nodes (x3 in both factors), a change of the starting
+ * values only -- the error estimate still accepts or rejects every step.  Every
+ * entry point honours it. */
+int accelerInt_set_stage_extrapolation(int mode);
 
 /* Like accelerInt_integrate, returning ACCELERINT_OK, ACCELERINT_ERR_SYSTEMS or an error. */
 int accelerInt_integrate_status(int NUM, double t_start, double t_end, double stepsize,

@@ -32,7 +32,7 @@ class _Config(ctypes.Structure):
     _fields_ = [("atol", ctypes.c_double), ("rtol", ctypes.c_double),
                 ("poles_re", ctypes.c_double * NRA), ("poles_im", ctypes.c_double * NRA),
                 ("res_re", ctypes.c_double * NRA), ("res_im", ctypes.c_double * NRA),
-                ("max_steps", ctypes.c_int)]
+                ("max_steps", ctypes.c_int), ("stage_extrap", ctypes.c_int)]
 
 
 _POLES = None
@@ -114,10 +114,11 @@ class Oracle:
         self.lib.or_complex_inverse_hessenberg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _ip]
         self.lib.or_complex_inverse_hessenberg.restype = ctypes.c_int
 
-    def config(self, atol=1e-10, rtol=1e-6, poles=None, max_steps=0):
+    def config(self, atol=1e-10, rtol=1e-6, poles=None, max_steps=0, stage_extrapolation=0):
         c = _Config()
         c.atol, c.rtol = atol, rtol
         c.max_steps = max_steps
+        c.stage_extrap = stage_extrapolation
         p, r = poles if poles is not None else cf_poles(1e-10)
         for i in range(NRA):
             c.poles_re[i], c.poles_im[i] = p[i].real, p[i].imag
@@ -125,12 +126,13 @@ class Oracle:
         return c
 
     def integrate(self, solver, mech, y, var, t0, t1, atol=1e-10, rtol=1e-6, nthreads=0, poles=None,
-                  fd_jacobian=False, max_steps=0):
+                  fd_jacobian=False, max_steps=0, stage_extrapolation=0):
         """One global step [t0, t1] for every system.  Returns (y_new, codes, stats[num, NSTATS]).
-        max_steps: Radau step limit (0: the reference's 200000)."""
+        max_steps: Radau step limit (0: the reference's 200000).  stage_extrapolation: Radau
+        starting values, 0 the reference's, 1 the collocation polynomial at all three nodes."""
         keep = []
         m = _mech_struct(mech, keep, (atol, rtol) if fd_jacobian else None)
-        c = self.config(atol, rtol, poles, max_steps)
+        c = self.config(atol, rtol, poles, max_steps, stage_extrapolation)
         y = np.array(y, dtype=np.float64, order="C", copy=True)
         num = y.shape[1]
         var = np.ascontiguousarray(var, dtype=np.float64)

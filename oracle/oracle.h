@@ -53,6 +53,10 @@ typedef struct {
      * A tight-tolerance oracle run raises it: at rtol 1e-12 a few ignition systems
      * take more steps than the reference allows at its own tolerance. */
     int max_steps;
+    /* Radau starting values after an accepted step: 0 the reference's (radau2a.c:312,
+     * x2 in the outer factor of Z3); 1 the collocation polynomial at all three nodes
+     * (x3 there), the library's accelerInt_set_stage_extrapolation(1). */
+    int stage_extrap;
 } or_config;
 
 /* Per-system counters; one row of OR_NSTATS doubles per system. */

@@ -107,17 +107,20 @@ static void make_interpolate(int n, const double* Z1, const double* Z2, const do
     }
 }
 
-/* radau2a.c:302-314; Z3 uses x2 in the outer factor exactly as the reference does */
-static void interpolate(int n, double H, double Hold, double* Z1, double* Z2, double* Z3, const double* CONT)
+/* radau2a.c:302-314; Z3 uses x2 in the outer factor exactly as the reference does
+ * (colloc = 0), or x3 (colloc = 1: the collocation polynomial at the third node) */
+static void interpolate(int n, double H, double Hold, double* Z1, double* Z2, double* Z3, const double* CONT,
+                        int colloc)
 {
     double r = H / Hold;
     double x1 = 1.0 + rkC[0] * r;
     double x2 = 1.0 + rkC[1] * r;
     double x3 = 1.0 + rkC[2] * r;
+    double x3o = colloc ? x3 : x2;
     for (int i = 0; i < n; i++) {
         Z1[i] = CONT[i] + x1 * (CONT[n + i] + x1 * CONT[n + n + i]);
         Z2[i] = CONT[i] + x2 * (CONT[n + i] + x2 * CONT[n + n + i]);
-        Z3[i] = CONT[i] + x2 * (CONT[n + i] + x3 * CONT[n + n + i]);
+        Z3[i] = CONT[i] + x3o * (CONT[n + i] + x3 * CONT[n + n + i]);
     }
 }
 
@@ -257,7 +260,7 @@ int or_radau2a(const or_config* c, const or_mech* m, double t_start, double t_en
             memset(Z2, 0, n * sizeof(double));
             memset(Z3, 0, n * sizeof(double));
         } else {
-            interpolate(n, H, Hold, Z1, Z2, Z3, CONT);
+            interpolate(n, H, Hold, Z1, Z2, Z3, CONT, c->stage_extrap);
         }
         bool NewtonDone = false;
         double NewtonIncrementOld = 0;

@@ -93,6 +93,11 @@ def test_extension_setters_validate_without_a_device():
     assert lib.accelerInt_get_mapping(ctypes.byref(tl), ctypes.byref(gr), None) == 0
     assert (tl.value, gr.value) == (16, 4)
     assert lib.accelerInt_set_mapping(0, 1) == 0
+    # Radau starting values: 0 the reference's, 1 collocation
+    assert lib.accelerInt_set_stage_extrapolation(2) == -1
+    assert lib.accelerInt_set_stage_extrapolation(-1) == -1
+    assert lib.accelerInt_set_stage_extrapolation(1) == 0
+    assert lib.accelerInt_set_stage_extrapolation(0) == 0
     # learned proposals: unknown flags, missing buffers, not initialised
     assert lib.accelerInt_set_learned(None, None, 4) == -1
     assert lib.accelerInt_set_learned(None, None, 1) == -1
