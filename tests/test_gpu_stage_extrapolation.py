@@ -26,12 +26,20 @@ TIGHT = os.path.join(os.path.dirname(__file__), "golden", "tight", "ma54_tight.n
 
 
 def _gpu(mech, y, var, t_end, dt, lu, mode):
-    integ = A.Integrator(y.shape[1], mech, lu=lu, stage_extrapolation=mode)
+    """Device-buffer path with the per-system counters: (y_out, codes, stats[num, NSTATS])."""
+    import torch
+    num = y.shape[1]
+    integ = A.Integrator(num, mech, lu=lu, stage_extrapolation=mode)
     try:
-        yo, codes, stats = integ.integrate(0.0, t_end, dt, y, var)
+        yd = torch.from_numpy(np.ascontiguousarray(y)).cuda()
+        vd = torch.from_numpy(np.ascontiguousarray(var)).cuda()
+        codes = torch.zeros(num, dtype=torch.int32, device="cuda")
+        stats = torch.zeros((num, A.NSTATS), dtype=torch.int32, device="cuda")
+        integ.integrate_device(0.0, t_end, dt, yd, vd, codes, stats)
+        torch.cuda.synchronize()
+        return yd.cpu().numpy(), codes.cpu().numpy(), stats.cpu().numpy()
     finally:
         integ.close()
-    return yo, codes, stats
 
 
 def _parity(oracle, mech, y, var, t_end, dt, name):
